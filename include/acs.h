@@ -1,0 +1,172 @@
+/*
+ * acs.h -- C ABI of the B200 artificial-compressibility (AC) pseudo-time solver.
+ *
+ * Drop-in for the pseudo-time loop of the Fortran reference (paths relative to the reference
+ * project, OpenMp_Multicore/):
+ *   solve_U   equations.f90:244-301   ->  acs_solve_u
+ *   solve_V   equations.f90:546-603   ->  acs_solve_v
+ *   solve_P   equations.f90:607-665   ->  acs_solve_p
+ *   solve_Z   equations.f90:669-719   ->  acs_solve_z
+ *   solve_C   equations.f90:769-819   ->  acs_solve_c
+ *   bcUV/bcP/bcZ/bcC boundary.f90:1-159 (called inside the routines above, as in the reference)
+ *   pseudo loop + convergence check main.f90:116-186 -> acs_physical_steps / acs_batch_run
+ *   mesh      nonsymetric_mesh.f90:1-218 -> acs_mesh_reference (driver-side helper)
+ *
+ * Conventions (those of the Fortran caller):
+ *   - every field is a caller-owned host array in Fortran order (column-major, i fastest):
+ *       um, um_tau, um_n_tau : (imax+1) x jmax
+ *       vm, vm_tau, vm_n_tau : imax x (jmax+1)
+ *       p, pn, T, T_*, C, C_*: imax x jmax
+ *   - 1-D metric arrays: x[imax], y[jmax], xm[imax+1], ym[jmax+1] (Fortran x(1) is x[0]);
+ *   - return value 0 = ACS_OK, otherwise an ACS_E_* code; no exception crosses the ABI;
+ *     acs_last_error() gives a message for the calling thread;
+ *   - a handle is used by one host thread at a time.
+ * All arithmetic is FP64.  Nothing here falls back to the CPU: without a CUDA device every
+ * call that needs one returns ACS_E_CUDA.
+ */
+#ifndef ACS_H
+#define ACS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum acs_status {
+  ACS_OK = 0,
+  ACS_E_ARG = 1,         /* null pointer or invalid parameter */
+  ACS_E_SIZE = 2,        /* grid too small/large, or size over a stated maximum */
+  ACS_E_CUDA = 3,        /* CUDA runtime error or no device */
+  ACS_E_NOMEM = 4,       /* device allocation failed */
+  ACS_E_STATE = 5,       /* call out of order */
+  ACS_E_UNSUPPORTED = 6  /* option not available for this input */
+};
+
+/* convection scheme */
+enum acs_scheme { ACS_SCHEME_QUICK = 0, ACS_SCHEME_UPWIND = 1 };
+/* boundary passes */
+enum acs_bc { ACS_BC_REFERENCE = 0, ACS_BC_CHANNEL = 1 };
+/* arithmetic: EXACT keeps the reference's operation order with every product and sum
+ * separately rounded (bit-identical to a -ffp-contract=off CPU build); FAST uses fused
+ * multiply-adds and precomputed reciprocals of the metric (results differ in the last bits). */
+enum acs_arith { ACS_ARITH_EXACT = 0, ACS_ARITH_FAST = 1 };
+
+/* per-case status word */
+enum acs_case_status { ACS_CASE_RUNNING = 0, ACS_CASE_DONE = 1, ACS_CASE_FAILED = 2 };
+
+/* Constants read by the loop (comum.f90:29-31, 79-85, 112-115; iterations.dat; main.f90:105-106).
+ * Same layout as the oracle's parameter block. */
+typedef struct acs_params {
+  int imax, jmax;      /* p-node counts (comum.f90:44-46) */
+  int scheme;          /* acs_scheme */
+  int bc;              /* acs_bc */
+  int solve_scalars;   /* 1: solve_Z and solve_C run inside the loop (main.f90:130-132) */
+  int itc_max;         /* pseudo-iteration cap per physical step (main.f90:120) */
+  double Re, Pe, Sc;   /* Reynolds, Peclet (T diffusion 1/Pe), Schmidt (C diffusion 1/(Re Sc)) */
+  double Da, Cf;       /* Darcy number, Forchheimer coefficient */
+  double g;            /* body force on u: RU -= g*epsilon1 (equations.f90:104) */
+  double InvFr2;       /* buoyancy: RV += InvFr2*(1 - 1/Tbar) (equations.f90:405) */
+  double v_in;         /* inflow velocity (v_i at the bottom for ACS_BC_REFERENCE, u on the left
+                          for ACS_BC_CHANNEL) */
+  double T_in;         /* T on the inflow boundary (Tinf, boundary.f90:86) */
+  double C_in;         /* C on the inflow boundary (0 in boundary.f90:129) */
+  double b_art;        /* artificial bulk viscosity */
+  double beta;         /* artificial compressibility */
+  double dt, dtau;     /* physical and pseudo time steps */
+  double eps;          /* tolerance on max(res_u, res_v, res_p) (main.f90:139-142) */
+  int arith;           /* acs_arith (solver option, no reference counterpart) */
+  int continuity;      /* 0: RP = -(face-flux balance) as in equations.f90:623-625;
+                          1: RP divided by the p-cell volume vol_p (nonsymetric_mesh.f90:234-238),
+                          i.e. the velocity divergence (used by the channel configurations) */
+} acs_params;
+
+/* Grid and porous fields (module comum: x, y, xm, ym, epsilon1, liga_poros). */
+typedef struct acs_grid {
+  int imax, jmax;
+  const double *x, *y, *xm, *ym;      /* [imax], [jmax], [imax+1], [jmax+1] */
+  const double *epsilon1, *liga_poros;/* [imax*jmax] column-major */
+} acs_grid;
+
+/* field identifiers for get/set (main.f90:15-20) */
+enum acs_field {
+  ACS_UM = 0, ACS_VM, ACS_UM_TAU, ACS_VM_TAU, ACS_UM_N_TAU, ACS_VM_N_TAU,
+  ACS_P, ACS_PN, ACS_T, ACS_T_TAU, ACS_T_N_TAU, ACS_C, ACS_C_TAU, ACS_C_N_TAU,
+  ACS_NFIELDS
+};
+
+typedef struct acs_handle acs_handle;  /* one case */
+typedef struct acs_batch acs_batch;    /* many independent cases in one launch */
+
+const char* acs_last_error(void);
+const char* acs_version(void);
+int acs_device_count(int* n);
+
+/* ---- mesh helper (the reference driver's `CALL mesh`, nonsymetric_mesh.f90:1-218) ---------- */
+/* jmax of the compiled-in reference domain for a given imax (comum.f90:40-46). */
+int acs_reference_jmax(int imax);
+/* Reference domain 12 x 20, y stretched (Py=1.6, Q=1), porous block x<=-4, y>=0.5 dilated by
+ * the flag rule; eps = porosity in flagged cells.  flag may be NULL. */
+int acs_mesh_reference(int imax, double porosity, double* x, double* y, double* xm, double* ym,
+                       int* flag, double* epsilon1, double* liga_poros);
+/* Channel domain [0,Lx] x [0,Ly]: uniform x, y = Ly/2 (1 + tanh(s(2xi-1))/tanh(s)); up to two
+ * rectangular porous blocks (box = {x0,x1,y0,y1}; NULL or x0 > x1 disables a block). */
+int acs_mesh_channel(int imax, int jmax, double Lx, double Ly, double s, const double* box1,
+                     const double* box2, double porosity, double* x, double* y, double* xm,
+                     double* ym, int* flag, double* epsilon1, double* liga_poros);
+/* Seeded uniform noise in [-amp, amp): splitmix64 of (seed, case, field, index). */
+double acs_noise(uint64_t seed, uint64_t case_id, uint64_t field, uint64_t index, double amp);
+
+/* ---- single case -------------------------------------------------------------------------- */
+int acs_create(const acs_grid* g, const acs_params* p, acs_handle** out);
+int acs_destroy(acs_handle* h);
+/* Launch on this cudaStream_t (NULL = the library's own stream). */
+int acs_set_stream(acs_handle* h, void* cuda_stream);
+
+/* Per-routine entry points: host arrays in, host arrays out (one H2D/D2H each call).
+ * solve_U: mirrors solve_U(um,vm,um_n,um_tau,vm_tau,um_n_tau,p,residual_u); like the reference,
+ * its boundary pass rewrites the boundary values of vm_tau (in/out). */
+int acs_solve_u(acs_handle* h, const double* um, const double* um_tau, double* vm_tau,
+                const double* p, double* um_n_tau, double* residual_u);
+/* solve_V(um,vm,vm_n,um_tau,vm_tau,vm_n_tau,p,T,residual_v); rewrites um_tau's boundary. */
+int acs_solve_v(acs_handle* h, const double* vm, double* um_tau, const double* vm_tau,
+                const double* p, const double* T, double* vm_n_tau, double* residual_v);
+/* solve_P(p,um_n,vm_n,pn,residual_p) */
+int acs_solve_p(acs_handle* h, const double* p, const double* um_n_tau, const double* vm_n_tau,
+                double* pn, double* residual_p);
+/* solve_Z(um_n,vm_n,Z,Z_n_tau,Z_tau): temperature, diffusion 1/Pe */
+int acs_solve_z(acs_handle* h, const double* um_n_tau, const double* vm_n_tau, const double* T,
+                double* T_n_tau, const double* T_tau);
+/* solve_C(um_n,vm_n,C,C_n_tau,C_tau): concentration, diffusion 1/(Re Sc) */
+int acs_solve_c(acs_handle* h, const double* um_n_tau, const double* vm_n_tau, const double* Cc,
+                double* C_n_tau, const double* C_tau);
+
+/* Device-resident loop state (main.f90:15-20). */
+int acs_set_field(acs_handle* h, int field, const double* host);
+int acs_get_field(acs_handle* h, int field, double* host);
+/* n_steps physical steps of main.f90:116-186 on the device, the whole pseudo loop in one CUDA
+ * graph.  *itc is the reference's pseudo counter carried across calls (1 before the first step).
+ * iters[n_steps] and err[n_steps] (may be NULL) receive each step's pseudo-iteration count and
+ * final max residual.  Returns ACS_OK, or ACS_E_STATE with *status = ACS_CASE_FAILED when the
+ * residual became NaN/Inf. */
+int acs_physical_steps(acs_handle* h, int n_steps, int* itc, int* iters, double* err, int* status);
+
+/* ---- batch of independent cases ----------------------------------------------------------- */
+int acs_batch_create(const acs_grid* grids, const acs_params* params, int n_cases, acs_batch** out);
+int acs_batch_destroy(acs_batch* b);
+int acs_batch_set_stream(acs_batch* b, void* cuda_stream);
+int acs_batch_set_field(acs_batch* b, int case_id, int field, const double* host);
+int acs_batch_get_field(acs_batch* b, int case_id, int field, double* host);
+/* Runs every case for n_steps physical steps in one graph launch; converged cases drop out of
+ * the launch through per-case masks.  itc[n_cases] in/out; iters/err are [n_cases*n_steps]
+ * (case-major, may be NULL); status[n_cases] (may be NULL). */
+int acs_batch_run(acs_batch* b, int n_steps, int* itc, int* iters, double* err, int* status);
+/* Number of kernel launches issued by the last acs_batch_run / acs_physical_steps. */
+int acs_batch_launch_count(acs_batch* b, long long* launches);
+int acs_launch_count(acs_handle* h, long long* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ACS_H */

@@ -1,0 +1,72 @@
+// acs_dev.cuh -- device data model shared by the solver kernels and the host orchestration.
+//
+// Every case lives in its own set of pitched FP64 buffers.  A node (i,j) of the reference's
+// 1-based Fortran arrays is stored at (i-1) + (j-1)*pitch for every field of the case, so um,
+// vm and the cell fields share one index and one row pitch (pitch >= imax+1, a multiple of 4
+// doubles so rows start on 32-byte boundaries).  The u family (um, um_tau, um_n_tau) rotates
+// through three buffers by role instead of being copied (main.f90:145-157 copies); the same
+// holds for v, T and C, and p/pn rotate through two.
+#pragma once
+#include <cstdint>
+
+namespace acs {
+
+enum Role { R_PHYS = 0, R_TAU = 1, R_NTAU = 2 };
+enum CaseFlags {
+  F_BUOY = 1,      // buoyancy term active (InvFr2 != 0 and T not identically 1)
+  F_BART = 2,      // b_art != 0
+  F_POROUS = 4,    // some cell has liga != 0
+  F_BINARY = 8,    // epsilon1/liga take only (1,0) and (phi,1): fast path may use a byte mask
+};
+
+struct CaseDev {
+  int nx, ny, pitch, flags;
+  int scheme, bc, solve_scalars, itc_max;
+  double Re, Pe, Sc, Da, Cf, g, InvFr2, v_in, T_in, C_in, b_art, beta, dt, dtau, eps;
+  double phi;                         // porosity of flagged cells when F_BINARY
+  const double *x, *y, *xm, *ym;      // 1-based: x[1..nx], y[1..ny], xm[1..nx+1], ym[1..ny+1]
+  const double *epsf, *liga;          // pitched cell fields
+  const uint8_t* mask;                // pitched porous mask (1 = porous), F_BINARY only
+  // fast-path metric tables (1-based like x); see kernels_fast.cu
+  const double* mx;                   // per-i table, stride MX_STRIDE
+  const double* my;                   // per-j table, stride MY_STRIDE
+  double* U[3];
+  double* V[3];
+  double* P[2];
+  double* T[3];
+  double* C[3];
+  double* S[2];                       // stage scratch (largest field shape)
+  long long n_elems;                  // pitch * (ny+1): doubles per buffer
+};
+
+// Mutable per-case control word (device).  Roles index into CaseDev::U/V/T/C/P.
+struct CaseCtl {
+  int ru[3], rv[3], rt[3], rc[3], rp[2];
+  int itc;          // the reference's pseudo counter (main.f90:77,150,182)
+  int step;         // physical steps completed in this run
+  int n_steps;      // physical steps requested
+  int k;            // pseudo-iterations in the current step
+  int active;       // 1 while the case still iterates
+  int status;       // acs_case_status
+  int copy_phys;    // 1: copy tau -> phys at the next control pass (itc_max exit)
+  unsigned long long res_u, res_v, res_p;  // max |res| as IEEE bits (non-negative doubles)
+  long long total_iters;
+};
+
+// Tile of the launch grid: case id and the 1-based origin of a 32 x 8 node block.
+struct Tile { int c, i0, j0, pad; };
+
+constexpr int TILE_X = 32;
+constexpr int TILE_Y = 8;
+
+__host__ __device__ inline long long lin(int i, int j, int pitch) {
+  return (long long)(i - 1) + (long long)(j - 1) * pitch;
+}
+
+// max of non-negative doubles through their bit patterns (NaN bits compare above +inf, so a
+// NaN residual wins and is reported).
+__device__ inline void atomic_max_nonneg(unsigned long long* slot, double v) {
+  atomicMax(slot, (unsigned long long)__double_as_longlong(v));
+}
+
+}  // namespace acs

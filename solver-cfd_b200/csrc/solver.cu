@@ -1,0 +1,813 @@
+// solver.cu -- host orchestration and the C ABI (include/acs.h).
+//
+// A batch owns one device allocation holding, per case, the metric arrays, the porous fields and
+// the rotating field buffers (see acs_dev.cuh), plus the case table, the control words and a
+// tile table covering every case.  One pseudo-iteration is a fixed sequence of launches over the
+// tile table (U stages, V stages, P, T stages, C stages, control).  acs_batch_run captures that
+// sequence once as the body of a CUDA graph WHILE node whose condition kernel keeps looping
+// while any case is active, so a whole multi-step run is one graph launch with no host round
+// trip.  A single case (acs_handle) is a batch of one.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/acs.h"
+#include "acs_dev.cuh"
+#include "fast.h"
+#include "kernels.h"
+
+namespace acs {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CU(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) return fail(ACS_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+namespace {
+
+constexpr int kMinN = 6;
+constexpr int kMaxN = 1 << 15;
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct FieldLoc { int family; int role; };  // family: 0 U, 1 V, 2 P, 3 T, 4 C
+FieldLoc field_loc(int f) {
+  switch (f) {
+    case ACS_UM: return {0, R_PHYS};
+    case ACS_UM_TAU: return {0, R_TAU};
+    case ACS_UM_N_TAU: return {0, R_NTAU};
+    case ACS_VM: return {1, R_PHYS};
+    case ACS_VM_TAU: return {1, R_TAU};
+    case ACS_VM_N_TAU: return {1, R_NTAU};
+    case ACS_P: return {2, 0};
+    case ACS_PN: return {2, 1};
+    case ACS_T: return {3, R_PHYS};
+    case ACS_T_TAU: return {3, R_TAU};
+    case ACS_T_N_TAU: return {3, R_NTAU};
+    case ACS_C: return {4, R_PHYS};
+    case ACS_C_TAU: return {4, R_TAU};
+    case ACS_C_N_TAU: return {4, R_NTAU};
+  }
+  return {-1, -1};
+}
+
+}  // namespace
+
+struct Batch {
+  int n = 0;
+  std::vector<acs_params> prm;
+  std::vector<CaseDev> hc;    // host copy of the case table
+  std::vector<CaseCtl> hk;    // host copy of the control words
+  std::vector<char> t_unity;  // T known to be identically 1 (the buoyancy term vanishes)
+  char* pool = nullptr;
+  size_t pool_bytes = 0;
+  CaseDev* dc = nullptr;
+  CaseCtl* dk = nullptr;
+  Tile* dtiles = nullptr;
+  int ntiles = 0;
+  int* d_nactive = nullptr;
+  long long* d_iter = nullptr;
+  int* d_iters = nullptr;
+  double* d_err = nullptr;
+  long long stats_cap = 0;
+  int* h_flag = nullptr;  // mapped host word for the host-polled loop
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_conditional = true;
+  bool use_fast = false;
+  FastPlan* fast = nullptr;
+  long long launches = 0;
+  long long body_kernels = 0;
+  int graph_steps = -1;  // n_steps the graph's loop bound was built for
+
+  ~Batch() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    if (fast) fast_destroy(fast);
+    if (pool) cudaFree(pool);
+    if (d_iters) cudaFree(d_iters);
+    if (d_err) cudaFree(d_err);
+    if (h_flag) cudaFreeHost(h_flag);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+
+  double* buf(int c, int family, int idx) const {
+    const CaseDev& d = hc[c];
+    switch (family) {
+      case 0: return d.U[idx];
+      case 1: return d.V[idx];
+      case 2: return d.P[idx];
+      case 3: return d.T[idx];
+      case 4: return d.C[idx];
+    }
+    return nullptr;
+  }
+  int role_index(int c, FieldLoc L) const {
+    const CaseCtl& k = hk[c];
+    switch (L.family) {
+      case 0: return k.ru[L.role];
+      case 1: return k.rv[L.role];
+      case 2: return k.rp[L.role];
+      case 3: return k.rt[L.role];
+      case 4: return k.rc[L.role];
+    }
+    return 0;
+  }
+};
+
+namespace {
+
+int validate(const acs_grid& g, const acs_params& p) {
+  if (!g.x || !g.y || !g.xm || !g.ym || !g.epsilon1 || !g.liga_poros) return fail(ACS_E_ARG, "null grid array");
+  if (g.imax != p.imax || g.jmax != p.jmax) return fail(ACS_E_ARG, "grid and params disagree on imax/jmax");
+  if (p.imax < kMinN || p.jmax < kMinN || p.imax > kMaxN || p.jmax > kMaxN)
+    return fail(ACS_E_SIZE, "imax and jmax must lie in [6, 32768]");
+  if (p.scheme != 0 && p.scheme != 1) return fail(ACS_E_ARG, "scheme must be 0 or 1");
+  if (p.bc != 0 && p.bc != 1) return fail(ACS_E_ARG, "bc must be 0 or 1");
+  if (p.arith != ACS_ARITH_EXACT && p.arith != ACS_ARITH_FAST) return fail(ACS_E_ARG, "arith must be 0 or 1");
+  if (p.itc_max < 2) return fail(ACS_E_ARG, "itc_max must be at least 2");
+  if (!(p.Re > 0) || !(p.Pe > 0) || !(p.Sc > 0) || !(p.Da > 0)) return fail(ACS_E_ARG, "Re, Pe, Sc, Da must be positive");
+  return ACS_OK;
+}
+
+// Binary porous structure (eps, liga) in {(1,0), (phi,1)} for one phi.
+bool binary_porosity(const acs_grid& g, double* phi) {
+  const size_t nc = (size_t)g.imax * g.jmax;
+  double ph = -1.0;
+  for (size_t q = 0; q < nc; ++q) {
+    const double e = g.epsilon1[q], l = g.liga_poros[q];
+    if (l == 0.0) {
+      if (e != 1.0) return false;
+    } else if (l == 1.0) {
+      if (ph < 0.0) ph = e;
+      if (e != ph || !(e > 0.0)) return false;
+    } else {
+      return false;
+    }
+  }
+  *phi = ph < 0.0 ? 1.0 : ph;
+  return true;
+}
+
+int field_dims(const CaseDev& d, int family, int* w, int* h) {
+  *w = family == 0 ? d.nx + 1 : d.nx;
+  *h = family == 1 ? d.ny + 1 : d.ny;
+  return 0;
+}
+
+int put(Batch& b, int c, int family, int idx, const double* host) {
+  const CaseDev& d = b.hc[c];
+  int w, h;
+  field_dims(d, family, &w, &h);
+  CU(cudaMemcpy2DAsync(b.buf(c, family, idx), (size_t)d.pitch * 8, host, (size_t)w * 8, (size_t)w * 8, h,
+                       cudaMemcpyHostToDevice, b.stream));
+  return ACS_OK;
+}
+
+int get(Batch& b, int c, int family, int idx, double* host) {
+  const CaseDev& d = b.hc[c];
+  int w, h;
+  field_dims(d, family, &w, &h);
+  CU(cudaMemcpy2DAsync(host, (size_t)w * 8, b.buf(c, family, idx), (size_t)d.pitch * 8, (size_t)w * 8, h,
+                       cudaMemcpyDeviceToHost, b.stream));
+  return ACS_OK;
+}
+
+bool all_ones(const double* a, size_t n) {
+  for (size_t q = 0; q < n; ++q)
+    if (a[q] != 1.0) return false;
+  return true;
+}
+
+int upload_field(Batch& b, int c, int field, const double* host) {
+  FieldLoc L = field_loc(field);
+  if (L.family < 0) return fail(ACS_E_ARG, "unknown field id");
+  if (field == ACS_T) b.t_unity[c] = all_ones(host, (size_t)b.hc[c].nx * b.hc[c].ny);
+  return put(b, c, L.family, b.role_index(c, L), host);
+}
+
+int download_field(Batch& b, int c, int field, double* host) {
+  FieldLoc L = field_loc(field);
+  if (L.family < 0) return fail(ACS_E_ARG, "unknown field id");
+  int r = get(b, c, L.family, b.role_index(c, L), host);
+  if (r) return r;
+  CU(cudaStreamSynchronize(b.stream));
+  return ACS_OK;
+}
+
+int refresh_flags(Batch& b) {
+  for (int c = 0; c < b.n; ++c) {
+    CaseDev& d = b.hc[c];
+    const acs_params& p = b.prm[c];
+    int f = d.flags & ~F_BUOY;
+    if (p.InvFr2 != 0.0 && (p.solve_scalars || !b.t_unity[c])) f |= F_BUOY;
+    if (f != d.flags) {
+      d.flags = f;
+      CU(cudaMemcpyAsync(b.dc + c, &d, sizeof(CaseDev), cudaMemcpyHostToDevice, b.stream));
+    }
+  }
+  return ACS_OK;
+}
+
+int push_ctl(Batch& b) {
+  CU(cudaMemcpyAsync(b.dk, b.hk.data(), sizeof(CaseCtl) * b.n, cudaMemcpyHostToDevice, b.stream));
+  return ACS_OK;
+}
+int pull_ctl(Batch& b) {
+  CU(cudaMemcpyAsync(b.hk.data(), b.dk, sizeof(CaseCtl) * b.n, cudaMemcpyDeviceToHost, b.stream));
+  CU(cudaStreamSynchronize(b.stream));
+  return ACS_OK;
+}
+
+void reset_roles(CaseCtl& k) {
+  for (int r = 0; r < 3; ++r) k.ru[r] = k.rv[r] = k.rt[r] = k.rc[r] = r;
+  k.rp[0] = 0;
+  k.rp[1] = 1;
+}
+
+int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch** out) {
+  if (!grids || !params || n <= 0 || !out) return fail(ACS_E_ARG, "null argument or n <= 0");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(ACS_E_CUDA, "no CUDA device");
+  for (int c = 0; c < n; ++c) {
+    int r = validate(grids[c], params[c]);
+    if (r) return r;
+  }
+  const bool fast = params[0].arith == ACS_ARITH_FAST;
+  for (int c = 1; c < n; ++c)
+    if ((params[c].arith == ACS_ARITH_FAST) != fast) return fail(ACS_E_ARG, "all cases of a batch must use one arith mode");
+
+  // Layout of the pool: [case table][control][tiles][counters] then per case
+  // [metrics][eps][liga][mask][U x3][V x3][P x2][T x3][C x3][S x2].
+  std::vector<size_t> off(n);
+  std::vector<size_t> sizes(n);
+  size_t total = 0;
+  for (int c = 0; c < n; ++c) {
+    const int nx = params[c].imax, ny = params[c].jmax;
+    const size_t ne = align_up(nx + 1, 4) * (size_t)(ny + 1);
+    size_t sz = align_up(sizeof(double) * (2 * nx + 2 * ny + 6), 256) + 2 * align_up(8 * ne, 256) +
+                align_up(ne, 256) + 16 * align_up(8 * ne, 256);
+    off[c] = total;
+    sizes[c] = sz;
+    total += align_up(sz, 256);
+  }
+  std::vector<Tile> tiles;
+  for (int c = 0; c < n; ++c)
+    for (int j0 = 1; j0 <= params[c].jmax + 1; j0 += TILE_Y)
+      for (int i0 = 1; i0 <= params[c].imax + 1; i0 += TILE_X) tiles.push_back({c, i0, j0, 0});
+  const size_t a_case = align_up(sizeof(CaseDev) * n, 256);
+  const size_t a_ctl = align_up(sizeof(CaseCtl) * n, 256);
+  const size_t a_tile = align_up(sizeof(Tile) * tiles.size(), 256);
+  const size_t head = a_case + a_ctl + a_tile + 256;
+
+  Batch* b = new Batch();
+  b->n = n;
+  b->prm.assign(params, params + n);
+  b->hc.resize(n);
+  b->hk.assign(n, CaseCtl{});
+  b->t_unity.assign(n, 0);
+  b->use_fast = fast;
+  b->pool_bytes = head + total;
+  cudaError_t e = cudaMalloc(&b->pool, b->pool_bytes);
+  if (e != cudaSuccess) {
+    delete b;
+    return fail(ACS_E_NOMEM, std::string("cudaMalloc of the case pool: ") + cudaGetErrorString(e));
+  }
+  e = cudaMemset(b->pool, 0, b->pool_bytes);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete b;
+    return fail(ACS_E_CUDA, std::string("batch set-up: ") + cudaGetErrorString(e));
+  }
+  b->own_stream = true;
+  char* p = b->pool;
+  b->dc = (CaseDev*)p;
+  b->dk = (CaseCtl*)(p + a_case);
+  b->dtiles = (Tile*)(p + a_case + a_ctl);
+  b->d_nactive = (int*)(p + a_case + a_ctl + a_tile);
+  b->d_iter = (long long*)(p + a_case + a_ctl + a_tile + 64);
+  b->ntiles = (int)tiles.size();
+  char* base = p + head;
+  std::vector<double> stage;
+  for (int c = 0; c < n; ++c) {
+    const acs_grid& g = grids[c];
+    const acs_params& pr = params[c];
+    const int nx = pr.imax, ny = pr.jmax;
+    const int pitch = (int)align_up(nx + 1, 4);
+    const size_t ne = (size_t)pitch * (ny + 1);
+    char* q = base + off[c];
+    CaseDev& d = b->hc[c];
+    std::memset(&d, 0, sizeof(d));
+    d.nx = nx; d.ny = ny; d.pitch = pitch;
+    d.scheme = pr.scheme; d.bc = pr.bc; d.solve_scalars = pr.solve_scalars; d.itc_max = pr.itc_max;
+    d.Re = pr.Re; d.Pe = pr.Pe; d.Sc = pr.Sc; d.Da = pr.Da; d.Cf = pr.Cf; d.g = pr.g;
+    d.InvFr2 = pr.InvFr2; d.v_in = pr.v_in; d.T_in = pr.T_in; d.C_in = pr.C_in; d.b_art = pr.b_art;
+    d.beta = pr.beta; d.dt = pr.dt; d.dtau = pr.dtau; d.eps = pr.eps;
+    d.n_elems = (long long)ne;
+    stage.assign(2 * nx + 2 * ny + 6, 0.0);
+    double* X = stage.data();
+    double* Y = X + (nx + 1);
+    double* XM = Y + (ny + 1);
+    double* YM = XM + (nx + 2);
+    for (int i = 1; i <= nx; ++i) X[i] = g.x[i - 1];
+    for (int j = 1; j <= ny; ++j) Y[j] = g.y[j - 1];
+    for (int i = 1; i <= nx + 1; ++i) XM[i] = g.xm[i - 1];
+    for (int j = 1; j <= ny + 1; ++j) YM[j] = g.ym[j - 1];
+    double* dm = (double*)q;
+    d.x = dm; d.y = dm + (nx + 1); d.xm = d.y + (ny + 1); d.ym = d.xm + (nx + 2);
+    CU(cudaMemcpy(dm, stage.data(), sizeof(double) * stage.size(), cudaMemcpyHostToDevice));
+    q += align_up(sizeof(double) * (2 * nx + 2 * ny + 6), 256);
+    double* deps = (double*)q; q += align_up(8 * ne, 256);
+    double* dliga = (double*)q; q += align_up(8 * ne, 256);
+    uint8_t* dmask = (uint8_t*)q; q += align_up(ne, 256);
+    std::vector<double> pe(ne, 1.0), pl(ne, 0.0);
+    std::vector<uint8_t> pm(ne, 0);
+    bool porous = false;
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const size_t s = (size_t)(i - 1) + (size_t)(j - 1) * nx;
+        const size_t t = (size_t)lin(i, j, pitch);
+        pe[t] = g.epsilon1[s];
+        pl[t] = g.liga_poros[s];
+        pm[t] = g.liga_poros[s] != 0.0;
+        porous |= g.liga_poros[s] != 0.0;
+      }
+    CU(cudaMemcpy(deps, pe.data(), 8 * ne, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(dliga, pl.data(), 8 * ne, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(dmask, pm.data(), ne, cudaMemcpyHostToDevice));
+    d.epsf = deps; d.liga = dliga; d.mask = dmask;
+    double phi = 1.0;
+    if (binary_porosity(g, &phi)) d.flags |= F_BINARY;
+    d.phi = phi;
+    if (pr.b_art != 0.0) d.flags |= F_BART;
+    if (porous) d.flags |= F_POROUS;
+    if (pr.InvFr2 != 0.0 && pr.solve_scalars) d.flags |= F_BUOY;
+    double** bufs[5] = {d.U, d.V, d.P, d.T, d.C};
+    const int counts[5] = {3, 3, 2, 3, 3};
+    for (int f = 0; f < 5; ++f)
+      for (int r = 0; r < counts[f]; ++r) {
+        bufs[f][r] = (double*)q;
+        q += align_up(8 * ne, 256);
+      }
+    d.S[0] = (double*)q; q += align_up(8 * ne, 256);
+    d.S[1] = (double*)q; q += align_up(8 * ne, 256);
+    reset_roles(b->hk[c]);
+  }
+  if (fast) {
+    int r = fast_create(b->hc, grids, params, &b->fast);
+    if (r) {
+      delete b;
+      return r;
+    }
+  }
+  e = cudaMemcpy(b->dc, b->hc.data(), sizeof(CaseDev) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->dk, b->hk.data(), sizeof(CaseCtl) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->dtiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    delete b;
+    return fail(ACS_E_CUDA, std::string("batch upload: ") + cudaGetErrorString(e));
+  }
+  *out = b;
+  return ACS_OK;
+}
+
+// ---- launch sequences --------------------------------------------------------------------------
+// solve_U: three stages, each followed by bcUV(stage array, vm_tau) (equations.f90:259-296)
+void seq_u(Batch& b) {
+  if (b.use_fast) { fast_u(b.fast, b.dc, b.dk, b.dtiles, b.ntiles, b.n, b.stream); b.launches += fast_u_launches(b.fast); return; }
+  for (int s = 1; s <= 3; ++s) {
+    launch_u_stage_exact(s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
+    launch_bc_uv(b.dc, b.dk, b.n, s - 1, b.stream);
+  }
+  b.launches += 6;
+}
+
+// solve_V: three stages, each followed by bcUV(um_tau, stage array) (equations.f90:561-598)
+void seq_v(Batch& b) {
+  if (b.use_fast) { fast_v(b.fast, b.dc, b.dk, b.dtiles, b.ntiles, b.n, b.stream); b.launches += fast_v_launches(b.fast); return; }
+  for (int s = 1; s <= 3; ++s) {
+    launch_v_stage_exact(s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
+    launch_bc_uv(b.dc, b.dk, b.n, 3 + s - 1, b.stream);
+  }
+  b.launches += 6;
+}
+
+// solve_P: the stages fuse pointwise; the intermediate bcP(pi) never reaches the interior
+void seq_p(Batch& b) {
+  if (b.use_fast) { fast_p(b.fast, b.dc, b.dk, b.dtiles, b.ntiles, b.n, b.stream); b.launches += fast_p_launches(b.fast); return; }
+  launch_p_exact(b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
+  launch_bc_cell(b.dc, b.dk, b.n, 0, b.stream);
+  b.launches += 2;
+}
+
+// solve_Z / solve_C: three stages, each followed by bcZ / bcC
+void seq_s(Batch& b, bool is_c) {
+  if (b.use_fast) { fast_s(b.fast, is_c, b.dc, b.dk, b.dtiles, b.ntiles, b.n, b.stream); b.launches += fast_s_launches(b.fast); return; }
+  const int w0 = is_c ? 4 : 1;
+  for (int s = 1; s <= 3; ++s) {
+    launch_s_stage_exact(is_c, s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
+    launch_bc_cell(b.dc, b.dk, b.n, w0 + s - 1, b.stream);
+  }
+  b.launches += 6;
+}
+
+bool any_scalars(const Batch& b) {
+  for (auto& p : b.prm)
+    if (p.solve_scalars) return true;
+  return false;
+}
+
+// one pseudo-iteration (main.f90:122-150) for every active case
+void seq_iteration(Batch& b) {
+  seq_u(b);
+  seq_v(b);
+  seq_p(b);
+  if (any_scalars(b)) {
+    seq_s(b, false);
+    seq_s(b, true);
+  }
+  k_control<<<b.n, 256, 0, b.stream>>>(b.dc, b.dk, b.d_iters, b.d_err, b.d_nactive);
+  b.launches += 1;
+}
+
+long long max_total_iterations(const Batch& b, int n_steps) {
+  long long m = 0;
+  for (auto& p : b.prm) m = std::max(m, (long long)p.itc_max * (long long)n_steps);
+  return m + 2;
+}
+
+int build_graph(Batch& b, int n_steps) {
+  if (b.gexec) { cudaGraphExecDestroy(b.gexec); b.gexec = nullptr; }
+  if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
+  const long long saved = b.launches;
+  if (b.graph_conditional && !getenv("ACS_NO_CONDITIONAL_GRAPH")) {
+    cudaGraph_t g;
+    CU(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNode_t node;
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+    if (e == cudaSuccess) {
+      cudaGraph_t body = np.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(b.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        const long long l0 = b.launches;
+        seq_iteration(b);
+        k_loop_cond<<<1, 1, 0, b.stream>>>(b.d_nactive, b.d_iter, max_total_iterations(b, n_steps), h);
+        b.body_kernels = b.launches - l0 + 1;
+        e = cudaStreamEndCapture(b.stream, &body);
+      }
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b.gexec, g, 0);
+    if (e == cudaSuccess) {
+      b.graph = g;
+      b.launches = saved;
+      return ACS_OK;
+    }
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    b.graph_conditional = false;  // fall back to the host-polled loop below
+  }
+  // host-polled: the graph holds one iteration plus a flag publish
+  if (!b.h_flag) CU(cudaHostAlloc(&b.h_flag, sizeof(int), cudaHostAllocMapped));
+  int* d_flag = nullptr;
+  CU(cudaHostGetDevicePointer(&d_flag, b.h_flag, 0));
+  cudaGraph_t g;
+  CU(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
+  const long long l0 = b.launches;
+  seq_iteration(b);
+  k_loop_flag<<<1, 1, 0, b.stream>>>(b.d_nactive, b.d_iter, d_flag);
+  b.body_kernels = b.launches - l0 + 1;
+  CU(cudaStreamEndCapture(b.stream, &g));
+  CU(cudaGraphInstantiate(&b.gexec, g, 0));
+  b.graph = g;
+  b.launches = saved;
+  return ACS_OK;
+}
+
+int run_batch(Batch& b, int n_steps, int* itc, int* iters, double* err, int* status) {
+  if (n_steps <= 0) return fail(ACS_E_ARG, "n_steps must be positive");
+  int r = refresh_flags(b);
+  if (r) return r;
+  const long long need = (long long)b.n * n_steps;
+  if (need > b.stats_cap) {
+    if (b.d_iters) cudaFree(b.d_iters);
+    if (b.d_err) cudaFree(b.d_err);
+    b.d_iters = nullptr;
+    b.d_err = nullptr;
+    CU(cudaMalloc(&b.d_iters, sizeof(int) * need));
+    CU(cudaMalloc(&b.d_err, sizeof(double) * need));
+    b.stats_cap = need;
+    if (b.gexec) { cudaGraphExecDestroy(b.gexec); b.gexec = nullptr; }
+    if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
+  }
+  for (int c = 0; c < b.n; ++c) {
+    CaseCtl& k = b.hk[c];
+    k.itc = itc ? itc[c] : 1;
+    k.step = 0;
+    k.n_steps = n_steps;
+    k.k = 0;
+    k.active = 1;
+    k.status = 0;
+    k.copy_phys = 0;
+    k.res_u = k.res_v = k.res_p = 0;
+    k.total_iters = 0;
+  }
+  r = push_ctl(b);
+  if (r) return r;
+  CU(cudaMemsetAsync(b.d_nactive, 0, 256, b.stream));
+  // the graph bakes in the loop bound; rebuild when n_steps changes the bound
+  if (!b.gexec || b.graph_steps != n_steps) {
+    r = build_graph(b, n_steps);
+    if (r) return r;
+    b.graph_steps = n_steps;
+  }
+  if (b.graph_conditional) {
+    CU(cudaGraphLaunch(b.gexec, b.stream));
+    CU(cudaStreamSynchronize(b.stream));
+  } else {
+    const long long cap = max_total_iterations(b, n_steps);
+    for (long long it = 0; it < cap; ++it) {
+      CU(cudaGraphLaunch(b.gexec, b.stream));
+      if ((it & 15) == 15) {
+        CU(cudaStreamSynchronize(b.stream));
+        if (*(volatile int*)b.h_flag == 0) break;
+      }
+    }
+    CU(cudaStreamSynchronize(b.stream));
+  }
+  long long iters_done = 0;
+  CU(cudaMemcpy(&iters_done, b.d_iter, sizeof(long long), cudaMemcpyDeviceToHost));
+  b.launches = iters_done * b.body_kernels;
+  r = pull_ctl(b);
+  if (r) return r;
+  if (iters) CU(cudaMemcpy(iters, b.d_iters, sizeof(int) * need, cudaMemcpyDeviceToHost));
+  if (err) CU(cudaMemcpy(err, b.d_err, sizeof(double) * need, cudaMemcpyDeviceToHost));
+  bool failed = false;
+  for (int c = 0; c < b.n; ++c) {
+    if (itc) itc[c] = b.hk[c].itc;
+    if (status) status[c] = b.hk[c].status;
+    failed |= b.hk[c].status == ACS_CASE_FAILED;
+    b.hk[c].active = 0;
+  }
+  CU(cudaMemsetAsync(b.d_iter, 0, sizeof(long long), b.stream));
+  r = push_ctl(b);
+  if (r) return r;
+  CU(cudaStreamSynchronize(b.stream));
+  if (failed) return fail(ACS_E_STATE, "a case failed: NaN or infinite residual");
+  return ACS_OK;
+}
+
+// Per-routine calls run one routine's launches on case 0 with identity roles.
+int begin_routine(Batch& b) {
+  CaseCtl& k = b.hk[0];
+  reset_roles(k);
+  k.active = 1;
+  k.res_u = k.res_v = k.res_p = 0;
+  return push_ctl(b);
+}
+
+int end_routine(Batch& b) {
+  CU(cudaStreamSynchronize(b.stream));
+  CU(cudaGetLastError());
+  int r = pull_ctl(b);
+  b.hk[0].active = 0;
+  if (!r) r = push_ctl(b);
+  if (!r) CU(cudaStreamSynchronize(b.stream));
+  return r;
+}
+
+double bits_to_double(unsigned long long v) {
+  double d;
+  std::memcpy(&d, &v, 8);
+  return d;
+}
+
+}  // namespace
+}  // namespace acs
+
+using acs::Batch;
+
+struct acs_batch { Batch* b; };
+struct acs_handle { Batch* b; };
+
+extern "C" {
+
+const char* acs_last_error(void) { return acs::g_err.c_str(); }
+const char* acs_version(void) { return "acs-b200 1.0 (sm_100a, FP64)"; }
+
+int acs_device_count(int* n) {
+  if (!n) return acs::fail(ACS_E_ARG, "null");
+  if (cudaGetDeviceCount(n) != cudaSuccess) {
+    *n = 0;
+    cudaGetLastError();
+  }
+  return ACS_OK;
+}
+
+int acs_batch_create(const acs_grid* grids, const acs_params* params, int n_cases, acs_batch** out) {
+  if (!out) return acs::fail(ACS_E_ARG, "null out");
+  Batch* b = nullptr;
+  int r = acs::create_batch(grids, params, n_cases, &b);
+  if (r) return r;
+  *out = new acs_batch{b};
+  return ACS_OK;
+}
+
+int acs_batch_destroy(acs_batch* h) {
+  if (!h) return ACS_OK;
+  delete h->b;
+  delete h;
+  return ACS_OK;
+}
+
+int acs_batch_set_stream(acs_batch* h, void* s) {
+  if (!h) return acs::fail(ACS_E_ARG, "null handle");
+  Batch& b = *h->b;
+  if (b.gexec) { cudaGraphExecDestroy(b.gexec); b.gexec = nullptr; }
+  if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
+  if (s) {
+    if (b.own_stream) cudaStreamDestroy(b.stream);
+    b.stream = (cudaStream_t)s;
+    b.own_stream = false;
+  }
+  return ACS_OK;
+}
+
+int acs_batch_set_field(acs_batch* h, int c, int field, const double* host) {
+  if (!h || !host) return acs::fail(ACS_E_ARG, "null argument");
+  if (c < 0 || c >= h->b->n) return acs::fail(ACS_E_ARG, "case id out of range");
+  return acs::upload_field(*h->b, c, field, host);
+}
+
+int acs_batch_get_field(acs_batch* h, int c, int field, double* host) {
+  if (!h || !host) return acs::fail(ACS_E_ARG, "null argument");
+  if (c < 0 || c >= h->b->n) return acs::fail(ACS_E_ARG, "case id out of range");
+  return acs::download_field(*h->b, c, field, host);
+}
+
+int acs_batch_run(acs_batch* h, int n_steps, int* itc, int* iters, double* err, int* status) {
+  if (!h) return acs::fail(ACS_E_ARG, "null handle");
+  return acs::run_batch(*h->b, n_steps, itc, iters, err, status);
+}
+
+int acs_batch_launch_count(acs_batch* h, long long* n) {
+  if (!h || !n) return acs::fail(ACS_E_ARG, "null");
+  *n = h->b->launches;
+  return ACS_OK;
+}
+
+int acs_create(const acs_grid* g, const acs_params* p, acs_handle** out) {
+  if (!out) return acs::fail(ACS_E_ARG, "null out");
+  Batch* b = nullptr;
+  int r = acs::create_batch(g, p, 1, &b);
+  if (r) return r;
+  *out = new acs_handle{b};
+  return ACS_OK;
+}
+
+int acs_destroy(acs_handle* h) {
+  if (!h) return ACS_OK;
+  delete h->b;
+  delete h;
+  return ACS_OK;
+}
+
+int acs_set_stream(acs_handle* h, void* s) {
+  if (!h) return acs::fail(ACS_E_ARG, "null handle");
+  acs_batch tmp{h->b};
+  return acs_batch_set_stream(&tmp, s);
+}
+
+int acs_set_field(acs_handle* h, int field, const double* host) {
+  if (!h || !host) return acs::fail(ACS_E_ARG, "null argument");
+  return acs::upload_field(*h->b, 0, field, host);
+}
+
+int acs_get_field(acs_handle* h, int field, double* host) {
+  if (!h || !host) return acs::fail(ACS_E_ARG, "null argument");
+  return acs::download_field(*h->b, 0, field, host);
+}
+
+int acs_physical_steps(acs_handle* h, int n_steps, int* itc, int* iters, double* err, int* status) {
+  if (!h || !itc) return acs::fail(ACS_E_ARG, "null argument");
+  int st = 0;
+  int r = acs::run_batch(*h->b, n_steps, itc, iters, err, &st);
+  if (status) *status = st;
+  return r;
+}
+
+int acs_launch_count(acs_handle* h, long long* n) {
+  if (!h || !n) return acs::fail(ACS_E_ARG, "null");
+  *n = h->b->launches;
+  return ACS_OK;
+}
+
+#define NEED(x) if (!(x)) return acs::fail(ACS_E_ARG, "null argument: " #x)
+
+int acs_solve_u(acs_handle* h, const double* um, const double* um_tau, double* vm_tau, const double* p,
+                double* um_n_tau, double* residual_u) {
+  NEED(h); NEED(um); NEED(um_tau); NEED(vm_tau); NEED(p); NEED(um_n_tau); NEED(residual_u);
+  Batch& b = *h->b;
+  int r = acs::refresh_flags(b);
+  if (!r) r = acs::begin_routine(b);
+  if (!r) r = acs::put(b, 0, 0, acs::R_PHYS, um);
+  if (!r) r = acs::put(b, 0, 0, acs::R_TAU, um_tau);
+  if (!r) r = acs::put(b, 0, 1, acs::R_TAU, vm_tau);
+  if (!r) r = acs::put(b, 0, 2, 1, p);
+  if (r) return r;
+  acs::seq_u(b);
+  r = acs::end_routine(b);
+  if (!r) r = acs::get(b, 0, 0, acs::R_NTAU, um_n_tau);
+  if (!r) r = acs::get(b, 0, 1, acs::R_TAU, vm_tau);
+  if (!r) { cudaStreamSynchronize(b.stream); *residual_u = acs::bits_to_double(b.hk[0].res_u); }
+  return r;
+}
+
+int acs_solve_v(acs_handle* h, const double* vm, double* um_tau, const double* vm_tau, const double* p,
+                const double* T, double* vm_n_tau, double* residual_v) {
+  NEED(h); NEED(vm); NEED(um_tau); NEED(vm_tau); NEED(p); NEED(T); NEED(vm_n_tau); NEED(residual_v);
+  Batch& b = *h->b;
+  b.t_unity[0] = acs::all_ones(T, (size_t)b.hc[0].nx * b.hc[0].ny);
+  int r = acs::refresh_flags(b);
+  if (!r) r = acs::begin_routine(b);
+  if (!r) r = acs::put(b, 0, 1, acs::R_PHYS, vm);
+  if (!r) r = acs::put(b, 0, 0, acs::R_TAU, um_tau);
+  if (!r) r = acs::put(b, 0, 1, acs::R_TAU, vm_tau);
+  if (!r) r = acs::put(b, 0, 2, 1, p);
+  if (!r) r = acs::put(b, 0, 3, acs::R_PHYS, T);
+  if (r) return r;
+  acs::seq_v(b);
+  r = acs::end_routine(b);
+  if (!r) r = acs::get(b, 0, 1, acs::R_NTAU, vm_n_tau);
+  if (!r) r = acs::get(b, 0, 0, acs::R_TAU, um_tau);
+  if (!r) { cudaStreamSynchronize(b.stream); *residual_v = acs::bits_to_double(b.hk[0].res_v); }
+  return r;
+}
+
+int acs_solve_p(acs_handle* h, const double* p, const double* um_n_tau, const double* vm_n_tau, double* pn,
+                double* residual_p) {
+  NEED(h); NEED(p); NEED(um_n_tau); NEED(vm_n_tau); NEED(pn); NEED(residual_p);
+  Batch& b = *h->b;
+  int r = acs::begin_routine(b);
+  if (!r) r = acs::put(b, 0, 2, 0, p);
+  if (!r) r = acs::put(b, 0, 0, acs::R_NTAU, um_n_tau);
+  if (!r) r = acs::put(b, 0, 1, acs::R_NTAU, vm_n_tau);
+  if (r) return r;
+  acs::seq_p(b);
+  r = acs::end_routine(b);
+  if (!r) r = acs::get(b, 0, 2, 1, pn);
+  if (!r) { cudaStreamSynchronize(b.stream); *residual_p = acs::bits_to_double(b.hk[0].res_p); }
+  return r;
+}
+
+static int solve_scalar(acs_handle* h, bool is_c, const double* um_n_tau, const double* vm_n_tau, const double* Z,
+                        double* Z_n_tau, const double* Z_tau) {
+  NEED(h); NEED(um_n_tau); NEED(vm_n_tau); NEED(Z); NEED(Z_n_tau); NEED(Z_tau);
+  Batch& b = *h->b;
+  const int fam = is_c ? 4 : 3;
+  int r = acs::begin_routine(b);
+  if (!r) r = acs::put(b, 0, 0, acs::R_NTAU, um_n_tau);
+  if (!r) r = acs::put(b, 0, 1, acs::R_NTAU, vm_n_tau);
+  if (!r) r = acs::put(b, 0, fam, acs::R_PHYS, Z);
+  if (!r) r = acs::put(b, 0, fam, acs::R_TAU, Z_tau);
+  if (r) return r;
+  acs::seq_s(b, is_c);
+  r = acs::end_routine(b);
+  if (!r) r = acs::get(b, 0, fam, acs::R_NTAU, Z_n_tau);
+  if (!r) { cudaError_t e = cudaStreamSynchronize(b.stream); if (e != cudaSuccess) return acs::fail(ACS_E_CUDA, cudaGetErrorString(e)); }
+  return r;
+}
+
+int acs_solve_z(acs_handle* h, const double* um_n_tau, const double* vm_n_tau, const double* T, double* T_n_tau,
+                const double* T_tau) {
+  return solve_scalar(h, false, um_n_tau, vm_n_tau, T, T_n_tau, T_tau);
+}
+
+int acs_solve_c(acs_handle* h, const double* um_n_tau, const double* vm_n_tau, const double* Cc, double* C_n_tau,
+                const double* C_tau) {
+  return solve_scalar(h, true, um_n_tau, vm_n_tau, Cc, C_n_tau, C_tau);
+}
+
+}  // extern "C"

@@ -1,0 +1,38 @@
+"""The C ABI: the library loads, exports every symbol include/acs.h declares, and its parameter
+block matches the oracle's layout.  No compute call is made here."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "acs.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(acs_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    L = pkg.lib()
+    names = _declared()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(pkg.EXPORTED) <= set(names)
+
+
+def test_param_block_layout_matches_oracle(pkg, orc):
+    a = [(n, t) for n, t in pkg.AcsParams._fields_]
+    b = [(n, t) for n, t in orc.OrcParams._fields_]
+    assert a == b
+    assert ctypes.sizeof(pkg.AcsParams) == ctypes.sizeof(orc.OrcParams)
+
+
+def test_version_and_errors_without_device(pkg):
+    L = pkg.lib()
+    assert b"sm_100a" in L.acs_version()
+    # invalid arguments are rejected before any device work
+    assert L.acs_create(None, None, None) != 0
+    assert L.acs_batch_create(None, None, 0, None) != 0
+    assert pkg.reference_jmax(51) == 84

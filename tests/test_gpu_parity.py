@@ -1,0 +1,172 @@
+"""CUDA path (EXACT arithmetic) against the CPU oracle, bit for bit, through the C ABI."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, fcopy, mask_dead
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand_state(pkg, nx, ny, seed):
+    rng = np.random.default_rng(seed)
+    st = pkg.configs.zero_state(nx, ny)
+    for k, a in st.items():
+        if k.startswith("T"):
+            a[:] = rng.uniform(0.5, 1.5, a.shape)
+        elif k.startswith("C"):
+            a[:] = rng.uniform(0.0, 1.0, a.shape)
+        elif k.startswith("p"):
+            a[:] = rng.uniform(-2.0, 2.0, a.shape)
+        else:
+            a[:] = rng.uniform(-1.0, 1.0, a.shape)
+    return st
+
+
+def _cases(pkg):
+    cfg = pkg.configs
+    out = []
+    prm, mesh, _, _, _ = cfg.reference_case(12)
+    out.append(("reference-12", prm, mesh))
+    prm, mesh, _, _, _ = cfg.reference_case(23, b_art=0.3)
+    out.append(("reference-23-bart", prm, mesh))
+    prm, mesh, _, _ = cfg.channel_case(33, 21, scheme=pkg.SCHEME_QUICK, block=cfg.centred_block(2, 1, 0.3),
+                                       porosity=0.4, Da=1e-3, Cf=0.55, Ri=1.0, scalars=True)
+    out.append(("channel-quick-porous", prm, mesh))
+    prm, mesh, _, _ = cfg.channel_case(29, 17, scheme=pkg.SCHEME_UPWIND, continuity=0)
+    out.append(("channel-upwind", prm, mesh))
+    return out
+
+
+@pytest.mark.parametrize("which", range(4))
+def test_routines_bit_exact(gpu, orc, which):
+    """solve_U/V/P/Z/C on random fields: every output array and residual bit-identical."""
+    pkg = gpu
+    name, prm, mesh = _cases(pkg)[which]
+    nx, ny = prm.imax, prm.jmax
+    g = pkg.Case(prm, mesh)
+    o = orc.OracleCase(prm, mesh)
+    for rep in range(2):
+        s = _rand_state(pkg, nx, ny, 10 * which + rep)
+        a, b = fcopy(s), fcopy(s)
+        ru_g = g.solve_U(a["um"], a["vm"], None, a["um_tau"], a["vm_tau"], a["um_n_tau"], a["pn"])
+        ru_o = o.solve_u(b["um"], b["um_tau"], b["vm_tau"], b["pn"], b["um_n_tau"])
+        rv_g = g.solve_V(a["um"], a["vm"], None, a["um_tau"], a["vm_tau"], a["vm_n_tau"], a["pn"], a["T"])
+        rv_o = o.solve_v(b["vm"], b["um_tau"], b["vm_tau"], b["pn"], b["T"], b["vm_n_tau"])
+        rp_g = g.solve_P(a["p"], a["um_n_tau"], a["vm_n_tau"], a["pn"])
+        rp_o = o.solve_p(b["p"], b["um_n_tau"], b["vm_n_tau"], b["pn"])
+        g.solve_Z(a["um_n_tau"], a["vm_n_tau"], a["T"], a["T_n_tau"], a["T_tau"])
+        o.solve_z(b["um_n_tau"], b["vm_n_tau"], b["T"], b["T_n_tau"], b["T_tau"])
+        g.solve_C(a["um_n_tau"], a["vm_n_tau"], a["C"], a["C_n_tau"], a["C_tau"])
+        o.solve_c(b["um_n_tau"], b["vm_n_tau"], b["C"], b["C_n_tau"], b["C_tau"])
+        assert (ru_g, rv_g, rp_g) == (ru_o, rv_o, rp_o), name
+        for k in ("um_n_tau", "vm_tau", "vm_n_tau", "um_tau", "pn", "T_n_tau", "C_n_tau"):
+            x, y = mask_dead(k, a[k], prm.bc), mask_dead(k, b[k], prm.bc)
+            assert np.array_equal(x, y), (name, k, float(np.nanmax(np.abs(x - y))))
+
+
+def _loop_compare(pkg, orc, prm, mesh, st, itc, nsteps):
+    g = pkg.Case(prm, mesh)
+    g.set_state(st)
+    itc_g, it_g, er_g, status = g.physical_steps(nsteps, itc)
+    out = g.get_state()
+    ost = fcopy(st)
+    itc_o, it_o, er_o = orc.OracleCase(prm, mesh).run(ost, nsteps, itc)
+    assert status == pkg.CASE_DONE
+    assert list(it_g) == list(it_o) and itc_g == itc_o
+    assert np.array_equal(er_g, er_o)
+    for k in pkg.FIELDS:
+        x, y = mask_dead(k, out[k], prm.bc), mask_dead(k, ost[k], prm.bc)
+        assert np.array_equal(x, y), (k, float(np.abs(x - y).max()))
+    assert g.launch_count() > 0
+    return it_g
+
+
+def test_loop_reference_small(gpu, orc):
+    prm, mesh, st, itc, _ = gpu.configs.reference_case(12, itc_max=5000)
+    it = _loop_compare(gpu, orc, prm, mesh, st, itc, 6)
+    assert it[0] >= 2
+
+
+def test_loop_channel_plain(gpu, orc):
+    """cfg-plain shape (51 x 51, upwind, beta=1) with the pseudo loop capped at 1500 per step."""
+    prm, mesh, st, itc, _ = gpu.configs.cfg_plain(itc_max=1500)
+    _loop_compare(gpu, orc, prm, mesh, st, itc, 2)
+
+
+def test_loop_channel_full_physics(gpu, orc):
+    """QUICK, porous block, buoyancy, both scalars; 2 steps of a 40 x 30 channel."""
+    cfg = gpu.configs
+    prm, mesh, st, itc = cfg.channel_case(40, 30, seed=3, Re=200.0, scheme=gpu.SCHEME_QUICK,
+                                          block=cfg.centred_block(2, 1, 0.3), porosity=0.4, Da=1e-3,
+                                          Cf=0.55, Ri=1.0, scalars=True, itc_max=1200)
+    _loop_compare(gpu, orc, prm, mesh, st, itc, 2)
+
+
+def test_batch_equals_oracle_per_case(gpu, orc):
+    """Ragged batch (sizes, schemes, both boundary variants, converging and capped cases) in one
+    graph launch; each case bit-identical to its own oracle run."""
+    cfg = gpu.configs
+    items = []
+    prm, mesh, st, itc, _ = cfg.reference_case(12, itc_max=4000)
+    items.append((prm, mesh, st, itc))
+    prm, mesh, st, itc, _ = cfg.reference_case(14, itc_max=4000, scheme=gpu.SCHEME_UPWIND)
+    items.append((prm, mesh, st, itc))
+    for c in range(4):
+        q = cfg.batch_case_params(c, 0, sizes=(17, 24, 31))
+        items.append(cfg.channel_case(q["nx"], q["ny"], seed=0, case_id=c, Re=q["Re"], block=q["block"],
+                                      porosity=q["porosity"], Da=q["Da"], Cf=0.55, Ri=q["Ri"],
+                                      scalars=True, itc_max=700))
+    b = gpu.Batch([x[0] for x in items], [x[1] for x in items])
+    for c, x in enumerate(items):
+        b.set_state(c, x[2])
+    nsteps = 3
+    itc_g, it_g, er_g, st_g = b.run(nsteps, [x[3] for x in items])
+    assert (st_g == gpu.CASE_DONE).all()
+    for c, (prm, mesh, st, itc) in enumerate(items):
+        ost = fcopy(st)
+        itc_o, it_o, er_o = orc.OracleCase(prm, mesh).run(ost, nsteps, itc)
+        assert list(it_g[c]) == list(it_o) and itc_g[c] == itc_o, c
+        out = b.get_state(c)
+        for k in gpu.FIELDS:
+            x, y = mask_dead(k, out[k], prm.bc), mask_dead(k, ost[k], prm.bc)
+            assert np.array_equal(x, y), (c, k)
+    assert b.launch_count() > 0
+
+
+def test_failed_case_is_isolated(gpu):
+    """A NaN in one case's input marks that case FAILED and leaves the others untouched."""
+    cfg = gpu.configs
+    prm, mesh, st, itc, _ = cfg.reference_case(12, itc_max=3000)
+    good = fcopy(st)
+    bad = fcopy(st)
+    bad["um_tau"][5, 7] = np.nan
+    b = gpu.Batch([prm, prm], [mesh, mesh])
+    b.set_state(0, good)
+    b.set_state(1, bad)
+    itc_g, it_g, er_g, status = b.run(3, [itc, itc])
+    assert status[0] == gpu.CASE_DONE and status[1] == gpu.CASE_FAILED
+    solo = gpu.Case(prm, mesh)
+    solo.set_state(good)
+    _, it_s, _, st_s = solo.physical_steps(3, itc)
+    assert list(it_s) == list(it_g[0])
+    a, c = solo.get_state(), b.get_state(0)
+    for k in ("um", "vm", "p"):
+        assert np.array_equal(a[k], c[k])
+
+
+def test_reference_run_51x84_matches_golden(gpu):
+    """The reference's default run (51 x 84, 200 steps, ~315k pseudo-iterations) on the GPU
+    against the end state written by the reference's OpenMP build."""
+    prm, mesh, st, itc, nsteps = gpu.configs.reference_case(51)
+    g = gpu.Case(prm, mesh)
+    g.set_state(st)
+    itc_g, it_g, er_g, status = g.physical_steps(nsteps, itc)
+    assert status == gpu.CASE_DONE
+    out = g.get_state()
+    ref = np.load(os.path.join(GOLDEN, "reference_51x84.npz"))
+    for k in ("um", "vm", "p", "T", "C"):
+        rel = np.abs(out[k] - ref[k]).max() / np.abs(ref[k]).max()
+        assert rel < 1e-12, (k, rel)
+    assert int(it_g.sum()) == 314712

@@ -1,0 +1,64 @@
+"""The product's host helpers (mesh, noise, case builders) against the oracle's restatement."""
+import numpy as np
+import pytest
+
+
+@pytest.mark.parametrize("imax", [10, 12, 26, 51, 102])
+def test_reference_mesh_bit_exact(pkg, orc, imax):
+    a, b = pkg.mesh_reference(imax), orc.mesh_reference(imax)
+    assert (a["nx"], a["ny"]) == (b["nx"], b["ny"])
+    for k in ("x", "y", "xm", "ym", "flag", "eps", "liga"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("nx,ny,block", [
+    (51, 51, None), (102, 102, (0.45, 1.55, 0.226, 0.774)), (37, 23, (0.0, 0.7, 0.3, 1.0)),
+    (64, 40, (1.3, 2.0, 0.0, 0.4))])
+def test_channel_mesh_bit_exact(pkg, orc, nx, ny, block):
+    a = pkg.mesh_channel(nx, ny, 2.0, 1.0, 1.5, block, 0.4)
+    b = orc.mesh_channel(nx, ny, 2.0, 1.0, 1.5, block, 0.4)
+    for k in ("x", "y", "xm", "ym", "flag", "eps", "liga"):
+        assert np.array_equal(a[k], b[k]), k
+    # tanh clustering toward the walls: the first and last y spacings are the smallest
+    dy = np.diff(a["y"])
+    assert dy[0] <= dy.min() * (1 + 1e-12) and dy[-1] < dy[len(dy) // 2]
+
+
+def test_noise_bit_exact(pkg, orc):
+    for args in [(0, 0, 1, 0), (1, 7, 2, 12345), (2**40, 255, 100, 3)]:
+        a = pkg.noise(*args, 1e-3)
+        assert a == orc.noise(*args, 1e-3)
+        assert -1e-3 <= a < 1e-3
+
+
+def test_block_area_and_batch_parameters(pkg):
+    cfg = pkg.configs
+    b = cfg.centred_block(2.0, 1.0, 0.3)
+    assert abs((b[1] - b[0]) * (b[3] - b[2]) - 0.6) < 1e-12
+    seen = set()
+    for c in range(64):
+        q = cfg.batch_case_params(c, 0)
+        assert q["nx"] in (51, 102, 153, 204) and q["ny"] in (51, 102, 153, 204)
+        assert 50 <= q["Re"] <= 500 and 1e-5 <= q["Da"] <= 1e-2
+        assert 0.3 <= q["porosity"] <= 0.9 and 0 <= q["Ri"] <= 2
+        x0, x1, y0, y1 = q["block"]
+        assert x0 >= -1e-12 and x1 <= 2 + 1e-12 and y0 >= -1e-12 and y1 <= 1 + 1e-12
+        seen.add((q["nx"], q["ny"]))
+    assert len(seen) > 8
+
+
+def test_reference_case_setup(pkg):
+    prm, mesh, st, itc, n = pkg.configs.reference_case(51)
+    assert (prm.imax, prm.jmax, itc, n) == (51, 84, 1, 200)
+    assert prm.beta == 1300.0 and prm.dtau == 0.05 and prm.dt == 0.005 and prm.eps == 1e-4
+    assert (st["vm"] == 5e-4).all() and (st["p"] == 1.0).all() and (st["pn"] == 0).all()
+    assert (st["T_tau"] == 0).all() and (st["C"][mesh["flag"] != 0] == 1.0).all()
+
+
+def test_channel_noise_only_on_update_region(pkg):
+    prm, mesh, st, itc, n = pkg.configs.cfg_plain()
+    um, vm = st["um"], st["vm"]
+    assert (um[:2, :] == 0).all() and (um[-2:, :] == 0).all() and (um[:, 0] == 0).all()
+    assert (vm[:, :2] == 0).all() and (vm[0, :] == 0).all()
+    assert 0 < np.abs(um).max() <= 1e-3 and 0 < np.abs(vm).max() <= 1e-3
+    assert n == 200 and prm.beta == 1.0 and prm.eps == 1e-6 and prm.continuity == 1
