@@ -22,6 +22,7 @@ enum CaseFlags {
 struct CaseDev {
   int nx, ny, pitch, flags;
   int scheme, bc, solve_scalars, itc_max;
+  int continuity, pad0;
   double Re, Pe, Sc, Da, Cf, g, InvFr2, v_in, T_in, C_in, b_art, beta, dt, dtau, eps;
   double phi;                         // porosity of flagged cells when F_BINARY
   const double *x, *y, *xm, *ym;      // 1-based: x[1..nx], y[1..ny], xm[1..nx+1], ym[1..ny+1]
@@ -42,6 +43,16 @@ struct CaseDev {
 // Mutable per-case control word (device).  Roles index into CaseDev::U/V/T/C/P.
 struct CaseCtl {
   int ru[3], rv[3], rt[3], rc[3], rp[2];
+  // Buffer holding the pressure that the momentum routines read (the reference's pn).  After a
+  // non-exit iteration the reference copies p = pn and keeps reading pn, so the latest pressure
+  // lives in both arrays; with swapped roles it lives only in the p-role buffer, rp[0].  After
+  // an exit (no copy) it is the pn-role buffer, rp[1].
+  int rp_read;
+  // What the reference's n_tau arrays hold after the last control pass: 0 = their own buffer,
+  // 1 = the same values as phys (after an exit, um = um_n_tau), 2 = the same values as tau
+  // (after a non-exit iteration, um_tau = um_n_tau).  The loop never reads n_tau before
+  // rewriting it, so this only matters when the state is read back.
+  int ntau_alias;
   int itc;          // the reference's pseudo counter (main.f90:77,150,182)
   int step;         // physical steps completed in this run
   int n_steps;      // physical steps requested
@@ -49,6 +60,7 @@ struct CaseCtl {
   int active;       // 1 while the case still iterates
   int status;       // acs_case_status
   int copy_phys;    // 1: copy tau -> phys at the next control pass (itc_max exit)
+  int scalars;      // 1: the T and C kernels run for this case
   unsigned long long res_u, res_v, res_p;  // max |res| as IEEE bits (non-negative doubles)
   long long total_iters;
 };

@@ -5,7 +5,9 @@
 //     IF (itc .NE. 1 .AND. error .LT. eps) EXIT                            (main.f90:142)
 // and applies the state updates of the reference by rotating buffer roles:
 //   * no exit: um_tau=um_n_tau, vm_tau=vm_n_tau, p=pn, T_tau=T_n_tau, C_tau=C_n_tau, itc+=1
-//     (main.f90:145-150) -> swap the tau and n_tau roles, swap p and pn;
+//     (main.f90:145-150) -> swap the tau and n_tau roles, swap p and pn; the momentum routines
+//     then read the pressure from the p-role buffer (CaseCtl::rp_read), since after the copy
+//     the reference's pn holds the same values;
 //   * exit: the tau copies are skipped (the next step starts from the previous pseudo-iterate,
 //     and p stays one iterate behind pn), then um=um_n_tau, vm=vm_n_tau, T=T_n_tau, C=C_n_tau
 //     and itc=0 (main.f90:154-157,182) -> swap the phys and n_tau roles;
@@ -46,6 +48,8 @@ __global__ void k_control(const CaseDev* __restrict__ cs, CaseCtl* __restrict__ 
         k.active = 0;
         step_done = true;
       } else if (k.itc != 1 && e < d.eps) {
+        k.rp_read = k.rp[1];
+        k.ntau_alias = 1;
         swap_i(k.ru[R_PHYS], k.ru[R_NTAU]);
         swap_i(k.rv[R_PHYS], k.rv[R_NTAU]);
         if (d.solve_scalars) {
@@ -57,6 +61,8 @@ __global__ void k_control(const CaseDev* __restrict__ cs, CaseCtl* __restrict__ 
         swap_i(k.ru[R_TAU], k.ru[R_NTAU]);
         swap_i(k.rv[R_TAU], k.rv[R_NTAU]);
         swap_i(k.rp[0], k.rp[1]);
+        k.rp_read = k.rp[0];
+        k.ntau_alias = 2;
         if (d.solve_scalars) {
           swap_i(k.rt[R_TAU], k.rt[R_NTAU]);
           swap_i(k.rc[R_TAU], k.rc[R_NTAU]);

@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(256) k_u_stage_exact(const CaseDev* __restrict
   const double* utau = d.U[k.ru[R_TAU]];
   const double* um = d.U[k.ru[R_PHYS]];
   const double* vt = d.V[k.rv[R_TAU]];
-  const double* pn = d.P[k.rp[1]];
+  const double* pn = d.P[k.rp_read];
   double a = 0.0;
   if (i >= 3 && i <= d.nx - 1 && j >= 2 && j <= d.ny - 1) {
     const bool quick = d.scheme == 0 && j >= 3 && j <= d.ny - 2;
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(256) k_v_stage_exact(const CaseDev* __restrict
   const double* vtau = d.V[k.rv[R_TAU]];
   const double* vm = d.V[k.rv[R_PHYS]];
   const double* ut = d.U[k.ru[R_TAU]];
-  const double* pn = d.P[k.rp[1]];
+  const double* pn = d.P[k.rp_read];
   const double* T = d.T[k.rt[R_PHYS]];
   double a = 0.0;
   if (i >= 2 && i <= d.nx - 1 && j >= 3 && j <= d.ny - 1) {
@@ -309,7 +309,8 @@ __global__ void __launch_bounds__(256) k_p_exact(const CaseDev* __restrict__ cs,
     const double Aew = g.ym[j + 1] - g.ym[j], Ans = g.xm[i + 1] - g.xm[i];
     const double dudx = un[g.o(i + 1, j)] * Aew - un[g.o(i, j)] * Aew;
     const double dvdy = vn[g.o(i, j + 1)] * Ans - vn[g.o(i, j)] * Ans;
-    const double RP = -(dudx + dvdy);
+    double RP = -(dudx + dvdy);
+    if (d.continuity == 1) RP = RP / ((g.ym[j + 1] - g.ym[j]) * (g.xm[i + 1] - g.xm[i]));
     const long long q = g.o(i, j);
     const double p0 = p[q];
     const double pi1 = p0 + d.dtau * RP * d.beta;
@@ -326,7 +327,7 @@ template <bool IS_C, int STAGE>
 __global__ void __launch_bounds__(256) k_s_stage_exact(const CaseDev* __restrict__ cs, CaseCtl* __restrict__ ctl,
                                                        const Tile* __restrict__ tiles) {
   const Tile t = tiles[blockIdx.x];
-  if (!ctl[t.c].active) return;
+  if (!ctl[t.c].active || !ctl[t.c].scalars) return;
   const CaseDev& d = cs[t.c];
   const CaseCtl& k = ctl[t.c];
   const G g(d);
@@ -454,6 +455,7 @@ __global__ void k_bc_cell(const CaseDev* __restrict__ cs, const CaseCtl* __restr
   const CaseDev& d = cs[c];
   const CaseCtl& k = ctl[c];
   if (which == 0) { bc_cell_block(d, d.P[k.rp[1]], true, 0.0); return; }
+  if (!k.scalars) return;
   const bool isC = which >= 4;
   const int s = isC ? which - 4 : which - 1;
   double* z = s == 2 ? (isC ? d.C[k.rc[R_NTAU]] : d.T[k.rt[R_NTAU]]) : d.S[s];

@@ -120,10 +120,12 @@ struct Batch {
   }
   int role_index(int c, FieldLoc L) const {
     const CaseCtl& k = hk[c];
+    if (L.role == R_NTAU && k.ntau_alias && (L.family <= 1 || hc[c].solve_scalars))
+      L.role = k.ntau_alias == 1 ? R_PHYS : R_TAU;
     switch (L.family) {
       case 0: return k.ru[L.role];
       case 1: return k.rv[L.role];
-      case 2: return k.rp[L.role];
+      case 2: return L.role == 1 ? k.rp_read : k.rp[0];
       case 3: return k.rt[L.role];
       case 4: return k.rc[L.role];
     }
@@ -142,6 +144,7 @@ int validate(const acs_grid& g, const acs_params& p) {
   if (p.bc != 0 && p.bc != 1) return fail(ACS_E_ARG, "bc must be 0 or 1");
   if (p.arith != ACS_ARITH_EXACT && p.arith != ACS_ARITH_FAST) return fail(ACS_E_ARG, "arith must be 0 or 1");
   if (p.itc_max < 2) return fail(ACS_E_ARG, "itc_max must be at least 2");
+  if (p.continuity != 0 && p.continuity != 1) return fail(ACS_E_ARG, "continuity must be 0 or 1");
   if (!(p.Re > 0) || !(p.Pe > 0) || !(p.Sc > 0) || !(p.Da > 0)) return fail(ACS_E_ARG, "Re, Pe, Sc, Da must be positive");
   return ACS_OK;
 }
@@ -164,6 +167,8 @@ bool binary_porosity(const acs_grid& g, double* phi) {
   *phi = ph < 0.0 ? 1.0 : ph;
   return true;
 }
+
+int push_ctl(Batch& b);
 
 int field_dims(const CaseDev& d, int family, int* w, int* h) {
   *w = family == 0 ? d.nx + 1 : d.nx;
@@ -198,6 +203,34 @@ bool all_ones(const double* a, size_t n) {
 int upload_field(Batch& b, int c, int field, const double* host) {
   FieldLoc L = field_loc(field);
   if (L.family < 0) return fail(ACS_E_ARG, "unknown field id");
+  if (L.role == R_NTAU && L.family != 2 && b.hk[c].ntau_alias) {
+    // give every n_tau array its own values again before one of them is overwritten
+    CaseCtl& k = b.hk[c];
+    const CaseDev& d = b.hc[c];
+    const int nfam = d.solve_scalars ? 4 : 2;
+    const int fams[4] = {0, 1, 3, 4};
+    for (int q = 0; q < nfam; ++q) {
+      const int f = fams[q];
+      const int src = b.role_index(c, FieldLoc{f, R_NTAU});
+      const int* roles = f == 0 ? k.ru : f == 1 ? k.rv : f == 3 ? k.rt : k.rc;
+      CU(cudaMemcpyAsync(b.buf(c, f, roles[R_NTAU]), b.buf(c, f, src), sizeof(double) * d.n_elems,
+                         cudaMemcpyDeviceToDevice, b.stream));
+    }
+    k.ntau_alias = 0;
+    int r = push_ctl(b);
+    if (r) return r;
+  }
+  if (L.family == 2) {
+    // p and pn share one buffer after a non-exit iteration; give pn its own buffer first
+    CaseCtl& k = b.hk[c];
+    if (k.rp_read == k.rp[0]) {
+      const CaseDev& d = b.hc[c];
+      CU(cudaMemcpyAsync(d.P[k.rp[1]], d.P[k.rp[0]], sizeof(double) * d.n_elems, cudaMemcpyDeviceToDevice, b.stream));
+      k.rp_read = k.rp[1];
+      int r = push_ctl(b);
+      if (r) return r;
+    }
+  }
   if (field == ACS_T) b.t_unity[c] = all_ones(host, (size_t)b.hc[c].nx * b.hc[c].ny);
   return put(b, c, L.family, b.role_index(c, L), host);
 }
@@ -239,6 +272,8 @@ void reset_roles(CaseCtl& k) {
   for (int r = 0; r < 3; ++r) k.ru[r] = k.rv[r] = k.rt[r] = k.rc[r] = r;
   k.rp[0] = 0;
   k.rp[1] = 1;
+  k.rp_read = 1;
+  k.ntau_alias = 0;
 }
 
 int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch** out) {
@@ -316,6 +351,7 @@ int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch**
     std::memset(&d, 0, sizeof(d));
     d.nx = nx; d.ny = ny; d.pitch = pitch;
     d.scheme = pr.scheme; d.bc = pr.bc; d.solve_scalars = pr.solve_scalars; d.itc_max = pr.itc_max;
+    d.continuity = pr.continuity;
     d.Re = pr.Re; d.Pe = pr.Pe; d.Sc = pr.Sc; d.Da = pr.Da; d.Cf = pr.Cf; d.g = pr.g;
     d.InvFr2 = pr.InvFr2; d.v_in = pr.v_in; d.T_in = pr.T_in; d.C_in = pr.C_in; d.b_art = pr.b_art;
     d.beta = pr.beta; d.dt = pr.dt; d.dtau = pr.dtau; d.eps = pr.eps;
@@ -533,6 +569,7 @@ int run_batch(Batch& b, int n_steps, int* itc, int* iters, double* err, int* sta
     k.copy_phys = 0;
     k.res_u = k.res_v = k.res_p = 0;
     k.total_iters = 0;
+    k.scalars = b.prm[c].solve_scalars ? 1 : 0;
   }
   r = push_ctl(b);
   if (r) return r;
@@ -584,6 +621,7 @@ int begin_routine(Batch& b) {
   CaseCtl& k = b.hk[0];
   reset_roles(k);
   k.active = 1;
+  k.scalars = 1;
   k.res_u = k.res_v = k.res_p = 0;
   return push_ctl(b);
 }
