@@ -1,0 +1,420 @@
+"""Benchmark: converged physical steps per second of the artificial-compressibility loop.
+
+A bench step is one converged physical step (a pseudo-time loop run to max residual < eps) of
+every case of the workload.  ``value`` is the whole-job throughput in converged physical steps
+per second with the state resident in HBM; ``e2e`` is the same metric through the C ABI with the
+state copied from pinned host buffers before and back after every step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--arith exact|fast]
+    python bench.py --impl reference ...   # the CPU implementation of the loop on host cores
+
+Multi-GPU (torchrun): each rank runs its own replica of the workload (cases are independent, so
+there is no exchange on the data path); the elapsed time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (description, bytes per cell-update of the fused model, config builder)
+    "full-102": "full equation set (u, v, p, T, C), QUICK, porous block 30% (porosity 0.4, Da 1e-3, Cf 0.55), "
+                "Ri 1, Pr 0.7, Sc 1, Re 200, 102 x 102 stretched 2:1 channel, beta 1, dt 1e-3, residual 1e-6",
+    "full-204": "as full-102 on a 204 x 204 mesh",
+    "plain-51": "plain method (u, v, p), first-order upwind, isothermal, no porous block, Re 100, 51 x 51 "
+                "stretched 2:1 channel, beta 1, dt 1e-3, residual 1e-6",
+    "batch-256": "256 independent cases, nx, ny in {51,102,153,204}, Re U[50,500], Da logU[1e-5,1e-2], "
+                 "porosity U[0.3,0.9], Ri U[0,2], random block position, full equation set, QUICK",
+}
+BYTES_PER_CELL_UPDATE = {"full": 204, "plain": 112}   # fused-kernel model, see DESIGN.md
+# per-node algorithmic bytes of the timed u-momentum kernel: reads u_in, um, um_tau, vm_tau, pn
+# (5 x 8 B) and the porous mask (1 B), writes u_out (8 B)
+U_KERNEL_BYTES = {"exact": 49, "fast": 41}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def build_workload(pkg, name, arith, seed_offset=0, max_iters=None):
+    items, kind = _build_workload(pkg, name, arith, seed_offset)
+    if max_iters:
+        from dataclasses import replace
+        items = [(replace(p, itc_max=max_iters),) + tuple(rest) for p, *rest in items]
+    return items, kind
+
+
+def _build_workload(pkg, name, arith, seed_offset=0):
+    cfg = pkg.configs
+    a = pkg.ARITH_FAST if arith == "fast" else pkg.ARITH_EXACT
+    if name == "batch-256":
+        items, _ = cfg.cfg_batch(256, seed=seed_offset, arith=a)
+        return items, "full"
+    if name.startswith("full-"):
+        n = int(name.split("-")[1])
+        prm, mesh, st, itc, _ = cfg.cfg_full(n, arith=a, seed=1 + seed_offset)
+        return [(prm, mesh, st, itc)], "full"
+    if name.startswith("plain-"):
+        n = int(name.split("-")[1])
+        prm, mesh, st, itc, _ = cfg.cfg_plain(n, arith=a, seed=seed_offset)
+        return [(prm, mesh, st, itc)], "plain"
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except OSError:
+            rows = []
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) >= 9:
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_sample(orc, items, gpu_iters_per_step, budget_s=12.0, threads=None):
+    """Time the oracle (the CPU implementation of the loop) on a bounded sample: for up to three
+    cases, a capped number of pseudo-iterations from the case's current state; extrapolate the
+    seconds per converged step with the pseudo-iteration counts of the GPU run (identical by
+    the parity tests)."""
+    import numpy as np
+    from dataclasses import replace
+    threads = threads or os.cpu_count() or 1
+    orc.set_threads(threads)
+    picks = sorted(range(len(items)), key=lambda c: items[c][0].imax * items[c][0].jmax)
+    picks = [picks[0], picks[len(picks) // 2], picks[-1]] if len(picks) > 3 else picks
+    per_cell_iter = []
+    sampled = 0
+    t_each = budget_s / len(picks)
+    for c in picks:
+        prm, mesh, st = items[c][0], items[c][1], items[c][2]
+        cells = prm.imax * prm.jmax
+        # size the sample to ~t_each seconds from a short probe
+        probe = 20
+        o = orc.OracleCase(replace(prm, itc_max=probe), mesh)
+        s = {k: np.asfortranarray(v.copy()) for k, v in st.items()}
+        t0 = time.perf_counter(); o.run(s, 1, 0); dt = time.perf_counter() - t0
+        m = max(20, int(t_each / max(dt / probe, 1e-9)))
+        o = orc.OracleCase(replace(prm, itc_max=m), mesh)
+        t0 = time.perf_counter(); _, it, _ = o.run(s, 1, 0); dt = time.perf_counter() - t0
+        per_cell_iter.append(dt / (int(it[0]) * cells))
+        sampled += int(it[0])
+    t_cell = statistics.mean(per_cell_iter)
+    sec_per_step = sum(gpu_iters_per_step[c] * items[c][0].imax * items[c][0].jmax * t_cell
+                       for c in range(len(items)))
+    return {"steps_per_s": len(items) / sec_per_step, "cores": threads,
+            "sample": f"{sampled} pseudo-iterations of {len(picks)} case(s) of the workload from its "
+                      f"post-warm-up state; seconds per cell-iteration x the GPU run's pseudo-iterations "
+                      f"per converged step"}
+
+
+def run_product(args):
+    import numpy as np
+    import torch
+    import __graft_entry__ as entry
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    pkg = entry.load_package()
+    if pkg.device_count() < 1:
+        raise SystemExit("no CUDA device")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    items, kind = build_workload(pkg, args.workload, args.arith, seed_offset=rank, max_iters=args.max_iters)
+    batch = pkg.Batch([x[0] for x in items], [x[1] for x in items])
+    batch.set_stream(stream.cuda_stream)
+    for c, x in enumerate(items):
+        batch.set_state(c, x[2])
+    itc = np.array([x[3] for x in items], np.int32)
+    n_cases = len(items)
+    cells = sum(x[0].imax * x[0].jmax for x in items)
+    l2 = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+
+    for w in range(args.warmup):
+        itc, _, _, st = batch.run(1, itc)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    iters = np.zeros((n_cases, args.steps), np.int64)
+    launches = 0
+    t_ev0, t_ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        torch.cuda.synchronize()
+        t_ev0.record(stream)
+        for k in range(args.steps):
+            l2.fill_(float(k))
+            itc, it, _, st = batch.run(1, itc)
+            iters[:, k] = it[:, 0]
+            launches += batch.launch_count()
+        t_ev1.record(stream)
+        torch.cuda.synchronize()
+    elapsed = t_ev0.elapsed_time(t_ev1) / 1e3
+    if world > 1:
+        t = torch.tensor([elapsed], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    total_iters = int(iters.sum())
+    steps_done = n_cases * args.steps
+    capped = int(sum((iters[c] >= items[c][0].itc_max - 1).sum() for c in range(n_cases)))
+    if args.record_iterations and rank == 0:
+        with open(args.record_iterations, "w") as f:
+            json.dump({"workload": args.workload, "warmup": args.warmup, "steps": args.steps,
+                       "iterations": iters.tolist()}, f)
+    value = steps_done * world / elapsed
+
+    # dominant kernel, timed alone
+    ms_u, nodes_u = batch.time_kernel(0, reps=50)
+    peak, peak_kind = measured_peaks()
+    b_node = U_KERNEL_BYTES[args.arith]
+    achieved = b_node * nodes_u / (ms_u * 1e-3) / 1e9
+    b_cu = BYTES_PER_CELL_UPDATE[kind]
+    cell_updates = sum(iters[c].sum() * items[c][0].imax * items[c][0].jmax for c in range(n_cases))
+    loop_gbs = b_cu * cell_updates / elapsed / 1e9
+
+    # end to end through the C ABI with host buffers (pinned)
+    e2e_steps = max(1, min(args.steps, 3))
+    host = []
+    h2d = d2h = 0
+    for c in range(n_cases):
+        got = batch.get_state(c)
+        pinned = {}
+        for n, a in got.items():
+            t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+            v = t.numpy().reshape(a.shape, order="F")
+            v[...] = a
+            pinned[n] = (t, v)
+            h2d += a.nbytes
+            d2h += a.nbytes
+        host.append(pinned)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        for c in range(n_cases):
+            batch.set_state(c, {n: v for n, (t, v) in host[c].items()})
+        itc, _, _, _ = batch.run(1, itc)
+        for c in range(n_cases):
+            batch.get_state(c, out={n: v for n, (t, v) in host[c].items()})
+    torch.cuda.synchronize()
+    e2e_elapsed = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_elapsed], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_elapsed = float(t.item())
+    e2e = n_cases * e2e_steps * world / e2e_elapsed
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as orc
+        gips = [float(iters[c].mean()) for c in range(n_cases)]
+        state_items = [(x[0], x[1], batch.get_state(c), 0) for c, x in enumerate(items)]
+        cpu = cpu_sample(orc, state_items, gips, budget_s=args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": "converged physical steps/s at pseudo-time residual 1e-6",
+            "value": value,
+            "unit": "steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": elapsed / args.steps * 1e3,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded channel cases; no public dataset)",
+            "config": {
+                "workload": args.workload,
+                "description": WORKLOADS[args.workload],
+                "cases_per_gpu": n_cases,
+                "cells_per_gpu": cells,
+                "arith": args.arith,
+                "pseudo_iterations_per_step_mean": total_iters / steps_done,
+                "steps_capped_at_itc_max": capped,
+                "l2": "flushed (256 MB write) before every timed step",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            },
+            "cell_updates_per_s": cell_updates * world / elapsed,
+            "roofline": {
+                "bound": "hbm",
+                "kernel": "u-momentum " + ("stage" if args.arith == "exact" else "fused routine"),
+                "achieved": achieved,
+                "peak": peak,
+                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst)" if peak_kind == "measured" else "fallback",
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "bytes_per_node": b_node,
+                "nodes_per_launch": nodes_u,
+                "ms_per_launch": ms_u,
+                "traffic": None,
+            },
+            "loop_roofline": {
+                "bytes_per_cell_update": b_cu,
+                "achieved": loop_gbs,
+                "unit": "GB/s",
+                "frac": loop_gbs / peak,
+            },
+            "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = {"value": cpu["steps_per_s"], "unit": "steps/s", "cores": cpu["cores"],
+                                    "kind": "port", "sample": cpu["sample"]}
+        if args.traffic is not None:
+            line["roofline"]["traffic"] = args.traffic
+        print(json.dumps(line))
+    batch.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def reference_iterations(workload):
+    path = os.path.join(ROOT, "tests", "golden", "bench_iterations.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(workload)
+    except (OSError, ValueError):
+        return None
+
+
+def run_reference(args):
+    """The reference's CPU implementation of the loop (the oracle restatement: the Fortran
+    reference cannot be compiled without a Fortran compiler) on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np
+    import __graft_entry__ as entry
+    from oracle import oracle as orc
+    pkg = entry.load_package()
+    items, kind = build_workload(pkg, args.workload, args.arith, max_iters=args.max_iters)
+    rec = reference_iterations(args.workload)
+    if rec is None:
+        print(json.dumps({"impl": "reference", "unavailable": "tests/golden/bench_iterations.json lacks "
+                          f"pseudo-iteration counts for workload {args.workload}"}))
+        return
+    per_case = rec["mean_iterations_per_step"]
+    gips = per_case if isinstance(per_case, list) else [per_case] * len(items)
+    vals = []
+    t0 = time.perf_counter()
+    cpu = None
+    for k in range(args.warmup + args.steps):
+        cpu = cpu_sample(orc, items, gips, budget_s=max(2.0, args.cpu_seconds / max(1, args.steps)))
+        if k >= args.warmup:
+            vals.append(cpu["steps_per_s"])
+    value = statistics.mean(vals)
+    elapsed = time.perf_counter() - t0
+    line = {
+        "impl": "reference",
+        "metric": "converged physical steps/s at pseudo-time residual 1e-6",
+        "value": value,
+        "unit": "steps/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded channel cases; no public dataset)",
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload], "cases": len(items),
+                   "pseudo_iterations_per_step_mean": float(np.mean(gips)),
+                   "source_of_iteration_counts": "tests/golden/bench_iterations.json"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cpu["cores"], "kind": "port",
+                         "sample": cpu["sample"] + " (initial state of the workload)"},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": elapsed,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="product", choices=["product", "reference"])
+    ap.add_argument("--workload", default="full-102", choices=sorted(WORKLOADS))
+    ap.add_argument("--arith", default="exact", choices=["exact", "fast"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of the timed kernel")
+    ap.add_argument("--max-iters", type=int, default=None,
+                    help="cap the pseudo-iterations of every physical step (profiling runs; the steps "
+                         "are then not converged)")
+    ap.add_argument("--record-iterations", default=None,
+                    help="write the per-step pseudo-iteration counts of the run to this JSON file")
+    args = ap.parse_args()
+    if args.warmup < 0 or args.steps < 1:
+        raise SystemExit("bad --steps/--warmup")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_product(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -117,6 +117,9 @@ int acs_mesh_channel(int imax, int jmax, double Lx, double Ly, double s, const d
                      double* ym, int* flag, double* epsilon1, double* liga_poros);
 /* Seeded uniform noise in [-amp, amp): splitmix64 of (seed, case, field, index). */
 double acs_noise(uint64_t seed, uint64_t case_id, uint64_t field, uint64_t index, double amp);
+/* out[k] = acs_noise(seed, case_id, field, index[k], amp) for k < n. */
+int acs_noise_array(uint64_t seed, uint64_t case_id, uint64_t field, const uint64_t* index, long long n,
+                    double amp, double* out);
 
 /* ---- single case -------------------------------------------------------------------------- */
 int acs_create(const acs_grid* g, const acs_params* p, acs_handle** out);
@@ -162,6 +165,25 @@ int acs_batch_get_field(acs_batch* b, int case_id, int field, double* host);
  * the launch through per-case masks.  itc[n_cases] in/out; iters/err are [n_cases*n_steps]
  * (case-major, may be NULL); status[n_cases] (may be NULL). */
 int acs_batch_run(acs_batch* b, int n_steps, int* itc, int* iters, double* err, int* status);
+/* Measurement helper (no reference counterpart): times `reps` back-to-back launches of one
+ * kernel of the pseudo-iteration over every case of the batch with CUDA events on the batch's
+ * stream and writes the mean duration of one launch in milliseconds.  kernel: 0 = u-momentum
+ * (first stage, or the whole fused routine on the FAST path), 1 = v-momentum, 2 = pressure,
+ * 3 = temperature, 4 = concentration.  Only stage scratch is written (the pressure kernel's
+ * output buffer is saved and restored), so the loop state is unchanged.  *cells receives the
+ * nodes one launch updates. */
+int acs_batch_time_kernel(acs_batch* b, int kernel, int reps, double* ms_mean, long long* cells);
+
+/* Solver options (no reference counterpart). */
+enum acs_option {
+  ACS_OPT_ENGINE = 1,        /* 0 (default): persistent cluster engine, one thread-block cluster
+                                per case runs whole physical steps in one launch;
+                                1: CUDA graph of per-stage kernels with a device WHILE node */
+  ACS_OPT_NODES_PER_CTA = 2  /* engine: target nodes per CTA when sizing a case's cluster */
+};
+int acs_batch_set_option(acs_batch* b, int option, long long value);
+int acs_set_option(acs_handle* h, int option, long long value);
+
 /* Number of kernel launches issued by the last acs_batch_run / acs_physical_steps. */
 int acs_batch_launch_count(acs_batch* b, long long* launches);
 int acs_launch_count(acs_handle* h, long long* launches);

@@ -38,12 +38,15 @@ FIELD_ID = {n: k for k, n in enumerate(FIELDS)}
 
 EXPORTED = (
     "acs_last_error", "acs_version", "acs_device_count", "acs_reference_jmax",
-    "acs_mesh_reference", "acs_mesh_channel", "acs_noise", "acs_create", "acs_destroy",
+    "acs_mesh_reference", "acs_mesh_channel", "acs_noise", "acs_noise_array", "acs_create", "acs_destroy",
     "acs_set_stream", "acs_solve_u", "acs_solve_v", "acs_solve_p", "acs_solve_z", "acs_solve_c",
     "acs_set_field", "acs_get_field", "acs_physical_steps", "acs_batch_create",
     "acs_batch_destroy", "acs_batch_set_stream", "acs_batch_set_field", "acs_batch_get_field",
-    "acs_batch_run", "acs_batch_launch_count", "acs_launch_count",
+    "acs_batch_run", "acs_batch_launch_count", "acs_launch_count", "acs_batch_time_kernel",
+    "acs_batch_set_option", "acs_set_option",
 )
+OPT_ENGINE, OPT_NODES_PER_CTA = 1, 2
+ENGINE_CLUSTER, ENGINE_GRAPH = 0, 1
 
 
 class AcsError(RuntimeError):
@@ -97,6 +100,7 @@ def _declare(L):
                                    C.c_double, _D, _D, _D, _D, _I, _D, _D]
     L.acs_noise.argtypes = [C.c_uint64] * 4 + [C.c_double]
     L.acs_noise.restype = C.c_double
+    L.acs_noise_array.argtypes = [C.c_uint64] * 3 + [C.POINTER(C.c_uint64), C.c_longlong, C.c_double, _D]
     L.acs_create.argtypes = [C.POINTER(AcsGrid), C.POINTER(AcsParams), C.POINTER(V)]
     L.acs_destroy.argtypes = [V]
     L.acs_set_stream.argtypes = [V, V]
@@ -116,6 +120,9 @@ def _declare(L):
     L.acs_batch_run.argtypes = [V, C.c_int, _I, _I, _D, _I]
     L.acs_batch_launch_count.argtypes = [V, C.POINTER(C.c_longlong)]
     L.acs_launch_count.argtypes = [V, C.POINTER(C.c_longlong)]
+    L.acs_batch_time_kernel.argtypes = [V, C.c_int, C.c_int, _D, C.POINTER(C.c_longlong)]
+    L.acs_batch_set_option.argtypes = [V, C.c_int, C.c_longlong]
+    L.acs_set_option.argtypes = [V, C.c_int, C.c_longlong]
 
 
 def _check(code: int, where: str):
@@ -209,6 +216,14 @@ def noise(seed, case_id, field_id, index, amp) -> float:
     return lib().acs_noise(seed, case_id, field_id, index, amp)
 
 
+def noise_array(seed, case_id, field_id, index: np.ndarray, amp) -> np.ndarray:
+    idx = np.ascontiguousarray(index, dtype=np.uint64)
+    out = np.zeros(idx.size)
+    _check(lib().acs_noise_array(seed, case_id, field_id, idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                 idx.size, amp, out.ctypes.data_as(_D)), "acs_noise_array")
+    return out
+
+
 def field_shape(name: str, nx: int, ny: int):
     if name.startswith("um"):
         return (nx + 1, ny)
@@ -256,6 +271,9 @@ class Case:
 
     def set_stream(self, stream_ptr: int):
         _check(lib().acs_set_stream(self.h, C.c_void_p(stream_ptr)), "acs_set_stream")
+
+    def set_option(self, option: int, value: int):
+        _check(lib().acs_set_option(self.h, option, value), "acs_set_option")
 
     # -- per-routine entry points (equations.f90) --
     def solve_U(self, um, vm, um_n, um_tau, vm_tau, um_n_tau, p) -> float:
@@ -347,6 +365,9 @@ class Batch:
     def set_stream(self, stream_ptr: int):
         _check(lib().acs_batch_set_stream(self.h, C.c_void_p(stream_ptr)), "acs_batch_set_stream")
 
+    def set_option(self, option: int, value: int):
+        _check(lib().acs_batch_set_option(self.h, option, value), "acs_batch_set_option")
+
     def zeros(self, c, name):
         p = self.params[c]
         return np.zeros(field_shape(name, p.imax, p.jmax), order="F")
@@ -356,13 +377,14 @@ class Batch:
             _check(lib().acs_batch_set_field(self.h, c, FIELD_ID[n], _dp(np.asfortranarray(a))),
                    "acs_batch_set_field")
 
-    def get_state(self, c: int, names=FIELDS) -> dict:
-        out = {}
+    def get_state(self, c: int, names=FIELDS, out=None) -> dict:
+        """Download fields of case c (into the arrays of `out` when given)."""
+        res = {}
         for n in names:
-            a = self.zeros(c, n)
+            a = out[n] if out is not None else self.zeros(c, n)
             _check(lib().acs_batch_get_field(self.h, c, FIELD_ID[n], _dp(a)), "acs_batch_get_field")
-            out[n] = a
-        return out
+            res[n] = a
+        return res
 
     def run(self, n_steps: int, itc):
         """Advance every case n_steps physical steps.  Returns (itc[n], iters[n, n_steps],
@@ -382,6 +404,14 @@ class Batch:
         n = C.c_longlong(0)
         _check(lib().acs_batch_launch_count(self.h, C.byref(n)), "acs_batch_launch_count")
         return n.value
+
+    def time_kernel(self, kernel: int, reps: int = 20):
+        """Mean duration (ms) of one launch of a loop kernel and the nodes it updates."""
+        ms = C.c_double(0.0)
+        cells = C.c_longlong(0)
+        _check(lib().acs_batch_time_kernel(self.h, kernel, reps, C.byref(ms), C.byref(cells)),
+               "acs_batch_time_kernel")
+        return ms.value, cells.value
 
 
 from . import configs  # noqa: E402  (uses the names above)

@@ -26,12 +26,13 @@ NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-
 # source -> extra flags
 SOURCES = {
     "kernels_exact.cu": ["-fmad=false"],
+    "engine_exact.cu": ["-fmad=false"],
     "control.cu": ["-fmad=false"],
     "kernels_fast.cu": [],
     "solver.cu": [],
 }
 CXX_SOURCES = {"mesh.cpp": ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"]}
-HEADERS = ["acs_dev.cuh", "kernels.h", "fast.h"]
+HEADERS = ["acs_dev.cuh", "kernels.h", "fast.h", "engine.cuh", "engine_api.h", "points_exact.cuh"]
 
 
 def nvcc() -> str:

@@ -21,7 +21,7 @@ from dataclasses import replace
 import numpy as np
 
 from . import (ARITH_EXACT, BC_CHANNEL, SCHEME_QUICK, SCHEME_UPWIND, Params, field_shape,
-               mesh_channel, mesh_reference, noise, reference_jmax)
+               mesh_channel, mesh_reference, noise, noise_array, reference_jmax)
 
 # field ids of the noise generator (shared by specification with the oracle tests)
 NOISE_U, NOISE_V, NOISE_PARAM = 1, 2, 100
@@ -66,25 +66,41 @@ def centred_block(Lx, Ly, frac):
     return (0.5 * (Lx - w), 0.5 * (Lx + w), 0.5 * (Ly - h), 0.5 * (Ly + h))
 
 
+def stable_dtau(mesh, beta, dt, safety=0.85):
+    """Largest pseudo step the three-stage Runge-Kutta loop tolerates for the artificial-
+    compressibility (pressure-velocity) mode: with the volume-divided continuity its eigenvalues
+    are about +-i sqrt(beta dt) 2 sqrt(1/dx^2 + 1/dy^2) per unit pseudo time, and SSP-RK3 is
+    stable on the imaginary axis up to sqrt(3).  `safety` < 1 keeps a margin."""
+    dx = np.diff(mesh["x"]).min()
+    dy = np.diff(mesh["y"]).min()
+    lam = math.sqrt(beta * dt) * 2.0 * math.sqrt(1.0 / dx ** 2 + 1.0 / dy ** 2)
+    return float(np.float64(safety * math.sqrt(3.0) / lam).round(6))
+
+
 def channel_case(nx, ny, *, seed=0, case_id=0, Re=100.0, scheme=SCHEME_QUICK, block=None,
                  block2=None, porosity=1.0, Da=1.0, Cf=0.0, Ri=0.0, Pr=0.7, Sc=1.0,
-                 scalars=False, beta=1.0, dt=1.0e-3, dtau=0.2, eps=1.0e-6, itc_max=100000,
+                 scalars=False, beta=1.0, dt=1.0e-3, dtau=None, eps=1.0e-6, itc_max=100000,
                  noise_amp=1.0e-3, T_block=2.0, Lx=2.0, Ly=1.0, stretch=1.5, arith=ARITH_EXACT,
                  continuity=1):
-    """Channel configuration.  Returns (params, mesh, state, itc0)."""
+    """Channel configuration.  Returns (params, mesh, state, itc0).  dtau=None picks
+    stable_dtau() for the mesh."""
+    mesh = mesh_channel(nx, ny, Lx, Ly, stretch, block, porosity, block2)
+    if dtau is None:
+        dtau = stable_dtau(mesh, beta, dt)
     prm = Params(imax=nx, jmax=ny, scheme=scheme, bc=BC_CHANNEL, solve_scalars=int(scalars),
                  itc_max=itc_max, Re=Re, Pe=Re * Pr, Sc=Sc, Da=Da, Cf=Cf, g=0.0, InvFr2=Ri,
                  v_in=1.0, T_in=1.0, C_in=1.0, b_art=0.0, beta=beta, dt=dt, dtau=dtau, eps=eps,
                  arith=arith, continuity=continuity)
-    mesh = mesh_channel(nx, ny, Lx, Ly, stretch, block, porosity, block2)
     st = zero_state(nx, ny)
     um, vm = st["um"], st["vm"]
-    for j in range(2, ny):          # u update region i = 3..nx-1, j = 2..ny-1
-        for i in range(3, nx):
-            um[i - 1, j - 1] = noise(seed, case_id, NOISE_U, (i - 1) + (j - 1) * (nx + 1), noise_amp)
-    for j in range(3, ny):          # v update region i = 2..nx-1, j = 3..ny-1
-        for i in range(2, nx):
-            vm[i - 1, j - 1] = noise(seed, case_id, NOISE_V, (i - 1) + (j - 1) * nx, noise_amp)
+    # u update region i = 3..nx-1, j = 2..ny-1; v update region i = 2..nx-1, j = 3..ny-1;
+    # noise index = the Fortran linear index (i-1) + (j-1)*leading dimension
+    I, J = np.meshgrid(np.arange(3, nx), np.arange(2, ny), indexing="ij")
+    um[I - 1, J - 1] = noise_array(seed, case_id, NOISE_U, ((I - 1) + (J - 1) * (nx + 1)).ravel(),
+                                   noise_amp).reshape(I.shape)
+    I, J = np.meshgrid(np.arange(2, nx), np.arange(3, ny), indexing="ij")
+    vm[I - 1, J - 1] = noise_array(seed, case_id, NOISE_V, ((I - 1) + (J - 1) * nx).ravel(),
+                                   noise_amp).reshape(I.shape)
     porous = mesh["flag"] != 0
     st["T"][:] = 1.0
     st["T"][porous] = T_block if scalars else 1.0

@@ -36,7 +36,7 @@ struct CaseDev {
   double* P[2];
   double* T[3];
   double* C[3];
-  double* S[2];                       // stage scratch (largest field shape)
+  double* S[4];                       // stage scratch (largest field shape)
   long long n_elems;                  // pitch * (ny+1): doubles per buffer
 };
 
@@ -63,6 +63,10 @@ struct CaseCtl {
   int scalars;      // 1: the T and C kernels run for this case
   unsigned long long res_u, res_v, res_p;  // max |res| as IEEE bits (non-negative doubles)
   long long total_iters;
+  // 1 while um_tau / vm_tau may not satisfy the boundary passes (after an upload): the next
+  // iteration must run U and V in the reference's order with the full bcUV side effects
+  int tau_dirty, pad1;
+  unsigned long long slot[2][3];  // residual maxima of the persistent engine, by iteration parity
 };
 
 // Tile of the launch grid: case id and the 1-based origin of a 32 x 8 node block.

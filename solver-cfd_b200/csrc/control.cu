@@ -63,6 +63,7 @@ __global__ void k_control(const CaseDev* __restrict__ cs, CaseCtl* __restrict__ 
         swap_i(k.rp[0], k.rp[1]);
         k.rp_read = k.rp[0];
         k.ntau_alias = 2;
+        k.tau_dirty = 0;
         if (d.solve_scalars) {
           swap_i(k.rt[R_TAU], k.rt[R_NTAU]);
           swap_i(k.rc[R_TAU], k.rc[R_NTAU]);

@@ -16,6 +16,7 @@ void fast_u(FastPlan* f, const CaseDev* dc, CaseCtl* dk, const Tile* tiles, int 
 void fast_v(FastPlan* f, const CaseDev* dc, CaseCtl* dk, const Tile* tiles, int ntiles, int ncases, cudaStream_t s);
 void fast_p(FastPlan* f, const CaseDev* dc, CaseCtl* dk, const Tile* tiles, int ntiles, int ncases, cudaStream_t s);
 void fast_s(FastPlan* f, bool is_c, const CaseDev* dc, CaseCtl* dk, const Tile* tiles, int ntiles, int ncases, cudaStream_t s);
+void fast_timed(FastPlan* f, int kernel, const CaseDev* dc, CaseCtl* dk, const Tile* tiles, int ntiles, int ncases, cudaStream_t s);
 int fast_u_launches(const FastPlan* f);
 int fast_v_launches(const FastPlan* f);
 int fast_p_launches(const FastPlan* f);

@@ -15,220 +15,10 @@
 #include "acs_dev.cuh"
 #include "kernels.h"
 
+#include "points_exact.cuh"
+
 namespace acs {
-namespace {
-
-struct G {
-  const double *x, *y, *xm, *ym;
-  int p;
-  __device__ G(const CaseDev& d) : x(d.x), y(d.y), xm(d.xm), ym(d.ym), p(d.pitch) {}
-  __device__ long long o(int i, int j) const { return lin(i, j, p); }
-};
-
-__device__ inline double pos(double a) { return a > 0.0 ? a : 0.0; }
-
-// ---- RESU: QUICK interior (equations.f90:14-104) --------------------------------------------
-__device__ double resu_quick(const CaseDev& d, const G& g, const double* um, const double* vm,
-                             const double* p, int i, int j) {
-  const double e = d.epsf[g.o(i, j)], lg = d.liga[g.o(i, j)];
-  const double An = g.x[i] - g.x[i - 1], As = An, Ae = g.ym[j + 1] - g.ym[j], Aw = Ae;
-  double fn = 0.5 * (vm[g.o(i, j + 1)] + vm[g.o(i - 1, j + 1)]) * An / e;
-  double fs = 0.5 * (vm[g.o(i, j)] + vm[g.o(i - 1, j)]) * As / e;
-  double fe = 0.5 * (um[g.o(i + 1, j)] + um[g.o(i, j)]) * Ae / e;
-  double fw = 0.5 * (um[g.o(i, j)] + um[g.o(i - 1, j)]) * Aw / e;
-  double df = fe - fw + fn - fs;
-  double Dn = (e / d.Re) * An / (g.y[j + 1] - g.y[j]);
-  double Ds = (e / d.Re) * As / (g.y[j] - g.y[j - 1]);
-  double De = (e / d.Re) * Ae / (g.xm[i + 1] - g.xm[i]);
-  double Dw = (e / d.Re) * Aw / (g.xm[i] - g.xm[i - 1]);
-  double afw = fw > 0.0 ? 1.0 : 0.0, afe = fe > 0.0 ? 1.0 : 0.0;
-  double afn = fn > 0.0 ? 1.0 : 0.0, afs = fs > 0.0 ? 1.0 : 0.0;
-  double aw = Dw + 0.75 * afw * fw + 0.125 * afe * fe + 0.375 * (1.0 - afw) * fw;
-  double ae = De - 0.375 * afe * fe - 0.75 * (1.0 - afe) * fe - 0.125 * (1.0 - afw) * fw;
-  double as = Ds + 0.75 * afs * fs + 0.125 * afn * fn + 0.375 * (1.0 - afs) * fs;
-  double an = Dn - 0.375 * afn * fn - 0.75 * (1.0 - afn) * fn - 0.125 * (1.0 - afs) * fs;
-  double aww = -0.125 * afw * fw, aee = 0.125 * (1.0 - afe) * fe;
-  double ass = -0.125 * afs * fs, ann = 0.125 * (1.0 - afn) * fn;
-  double ap = aw + ae + as + an + aww + aee + ass + ann + df;
-  double uW = um[g.o(i - 1, j)], uWW = um[g.o(i - 2, j)], uE = um[g.o(i + 1, j)],
-         uEE = um[g.o(i + 2, j)], uS = um[g.o(i, j - 1)], uSS = um[g.o(i, j - 2)],
-         uN = um[g.o(i, j + 1)], uNN = um[g.o(i, j + 2)], uP = um[g.o(i, j)], vP = vm[g.o(i, j)];
-  double q_art = e * (p[g.o(i, j)] - p[g.o(i - 1, j)]) / (g.x[i] - g.x[i - 1]);
-  if (d.flags & F_BART) {
-    double dudxdx = Ae * (uE - uP) / (g.xm[i + 1] - g.xm[i]) - Aw * (uP - uW) / (g.xm[i] - g.xm[i - 1]);
-    double dxdvdy = Ae * (vm[g.o(i, j + 1)] - vm[g.o(i, j)]) / (g.ym[j + 1] - g.ym[j]) -
-                    Aw * (vm[g.o(i - 1, j + 1)] - vm[g.o(i - 1, j)]) / (g.ym[j + 1] - g.ym[j]);
-    q_art = q_art + -(d.b_art * (dudxdx + dxdvdy));
-  }
-  double r = 1.0 / (g.x[i] - g.x[i - 1]) / (g.y[j] - g.y[j - 1]) *
-                 (-(ap * uP) + aww * uWW + aw * uW + aee * uEE + ae * uE + ass * uSS + as * uS +
-                  ann * uNN + an * uN) -
-             q_art;
-  if (d.flags & F_POROUS)
-    r = r - e * (uP / (d.Re * d.Da) + d.Cf / sqrt(e * d.Da) * uP * sqrt(uP * uP + vP * vP)) * lg;
-  return r - d.g * e;
-}
-
-// ---- RESU: first-order upwind rows (upwind_Ui/upwind_Uj, equations.f90:133-174) ----------------
-__device__ double resu_upwind(const CaseDev& d, const G& g, const double* um, const double* vm,
-                              const double* p, int i, int j) {
-  const double e = d.epsf[g.o(i, j)], lg = d.liga[g.o(i, j)];
-  const double An = g.x[i] - g.x[i - 1], As = An, Ae = g.ym[j + 1] - g.ym[j], Aw = Ae;
-  double fn = 0.5 * (vm[g.o(i, j + 1)] + vm[g.o(i - 1, j + 1)]) * An / e;
-  double fs = 0.5 * (vm[g.o(i, j)] + vm[g.o(i - 1, j)]) * As / e;
-  double fe = 0.5 * (um[g.o(i + 1, j)] + um[g.o(i, j)]) * Ae / e;
-  double fw = 0.5 * (um[g.o(i, j)] + um[g.o(i - 1, j)]) * Aw / e;
-  double df = fe - fw + fn - fs;
-  double Dn = (e / d.Re) * An / (g.y[j + 1] - g.y[j]);
-  double Ds = (e / d.Re) * As / (g.y[j] - g.y[j - 1]);
-  double De = (e / d.Re) * Ae / (g.xm[i + 1] - g.xm[i]);
-  double Dw = (e / d.Re) * Aw / (g.xm[i] - g.xm[i - 1]);
-  double aw = Dw + pos(fw), as = Ds + pos(fs), ae = De + pos(-fe), an = Dn + pos(-fn);
-  double ap = aw + ae + as + an + df;
-  double uW = um[g.o(i - 1, j)], uE = um[g.o(i + 1, j)], uS = um[g.o(i, j - 1)],
-         uN = um[g.o(i, j + 1)], uP = um[g.o(i, j)], vP = vm[g.o(i, j)];
-  double q_art = e * (p[g.o(i, j)] - p[g.o(i - 1, j)]) / (g.x[i] - g.x[i - 1]);
-  if (d.flags & F_BART) {
-    double dudxdx = Ae * (uE - uP) / (g.xm[i + 1] - g.xm[i]) - Aw * (uP - uW) / (g.xm[i] - g.xm[i - 1]);
-    double dxdvdy = Ae * (vm[g.o(i, j + 1)] - vm[g.o(i, j)]) / (g.ym[j + 1] - g.ym[j]) -
-                    Aw * (vm[g.o(i - 1, j + 1)] - vm[g.o(i - 1, j)]) / (g.ym[j + 1] - g.ym[j]);
-    q_art = q_art - d.b_art * (dudxdx + dxdvdy);
-  }
-  double r = 1.0 / (g.x[i] - g.x[i - 1]) / (g.y[j] - g.y[j - 1]) *
-                 (-(ap * uP) + aw * uW + ae * uE + as * uS + an * uN) -
-             q_art;
-  if (d.flags & F_POROUS)
-    r = r - e * (uP / (d.Re * d.Da) + d.Cf / sqrt(e * d.Da) * uP * sqrt(uP * uP + vP * vP)) * lg;
-  return r - d.g * e;
-}
-
-// ---- RESV (equations.f90:317-408, upwind :436-477) -------------------------------------------
-__device__ inline double buoyancy(const CaseDev& d, const G& g, const double* T, int i, int j) {
-  return d.InvFr2 * (1.0 - 1.0 / ((T[g.o(i, j)] + T[g.o(i, j - 1)]) * 0.5));
-}
-
-__device__ double resv_quick(const CaseDev& d, const G& g, const double* um, const double* vm,
-                             const double* p, const double* T, int i, int j) {
-  const double e = d.epsf[g.o(i, j)], lg = d.liga[g.o(i, j)];
-  const double An = g.xm[i + 1] - g.xm[i], As = An, Ae = g.y[j] - g.y[j - 1], Aw = Ae;
-  double fn = 0.5 * (vm[g.o(i, j)] + vm[g.o(i, j + 1)]) * An / e;
-  double fs = 0.5 * (vm[g.o(i, j)] + vm[g.o(i, j - 1)]) * As / e;
-  double fe = 0.5 * (um[g.o(i + 1, j)] + um[g.o(i + 1, j - 1)]) * Ae / e;
-  double fw = 0.5 * (um[g.o(i, j)] + um[g.o(i, j - 1)]) * Aw / e;
-  double df = fe - fw + fn - fs;
-  double Dn = (e / d.Re) * An / (g.ym[j + 1] - g.ym[j]);
-  double Ds = (e / d.Re) * As / (g.ym[j] - g.ym[j - 1]);
-  double De = (e / d.Re) * Ae / (g.x[i + 1] - g.x[i]);
-  double Dw = (e / d.Re) * Aw / (g.x[i] - g.x[i - 1]);
-  double afw = fw > 0.0 ? 1.0 : 0.0, afe = fe > 0.0 ? 1.0 : 0.0;
-  double afn = fn > 0.0 ? 1.0 : 0.0, afs = fs > 0.0 ? 1.0 : 0.0;
-  double aw = Dw + 0.75 * afw * fw + 0.125 * afe * fe + 0.375 * (1.0 - afw) * fw;
-  double ae = De - 0.375 * afe * fe - 0.75 * (1.0 - afe) * fe - 0.125 * (1.0 - afw) * fw;
-  double as = Ds + 0.75 * afs * fs + 0.125 * afn * fn + 0.375 * (1.0 - afs) * fs;
-  double an = Dn - 0.375 * afn * fn - 0.75 * (1.0 - afn) * fn - 0.125 * (1.0 - afs) * fs;
-  double aww = -0.125 * afw * fw, aee = 0.125 * (1.0 - afe) * fe;
-  double ass = -0.125 * afs * fs, ann = 0.125 * (1.0 - afn) * fn;
-  double ap = aw + ae + as + an + aww + aee + ass + ann + df;
-  double vW = vm[g.o(i - 1, j)], vWW = vm[g.o(i - 2, j)], vE = vm[g.o(i + 1, j)],
-         vEE = vm[g.o(i + 2, j)], vS = vm[g.o(i, j - 1)], vSS = vm[g.o(i, j - 2)],
-         vN = vm[g.o(i, j + 1)], vNN = vm[g.o(i, j + 2)], vP = vm[g.o(i, j)], uP = um[g.o(i, j)];
-  double q_art = e * (p[g.o(i, j)] - p[g.o(i, j - 1)]) / (g.y[j] - g.y[j - 1]);
-  if (d.flags & F_BART) {
-    double dvdydy = An * (vN - vP) / (g.ym[j + 1] - g.ym[j]) - As * (vP - vS) / (g.ym[j] - g.ym[j - 1]);
-    double dydudx = An * (um[g.o(i + 1, j)] - um[g.o(i, j)]) / (g.xm[i + 1] - g.xm[i]) -
-                    As * (um[g.o(i + 1, j - 1)] - um[g.o(i, j - 1)]) / (g.xm[i + 1] - g.xm[i]);
-    q_art = q_art + -(d.b_art * (dydudx + dvdydy));
-  }
-  double r = 1.0 / (g.x[i] - g.x[i - 1]) / (g.y[j] - g.y[j - 1]) *
-                 (-(ap * vP) + aww * vWW + aw * vW + aee * vEE + ae * vE + ass * vSS + as * vS +
-                  ann * vNN + an * vN) -
-             q_art;
-  if (d.flags & F_BUOY) r = r + buoyancy(d, g, T, i, j);
-  if (d.flags & F_POROUS)
-    r = r - e * (vP / (d.Re * d.Da) + d.Cf / sqrt(e * d.Da) * vP * sqrt(uP * uP + vP * vP)) * lg;
-  return r;
-}
-
-__device__ double resv_upwind(const CaseDev& d, const G& g, const double* um, const double* vm,
-                              const double* p, const double* T, int i, int j) {
-  const double e = d.epsf[g.o(i, j)], lg = d.liga[g.o(i, j)];
-  const double An = g.xm[i + 1] - g.xm[i], As = An, Ae = g.y[j] - g.y[j - 1], Aw = Ae;
-  double fn = 0.5 * (vm[g.o(i, j)] + vm[g.o(i, j + 1)]) * An / e;
-  double fs = 0.5 * (vm[g.o(i, j)] + vm[g.o(i, j - 1)]) * As / e;
-  double fe = 0.5 * (um[g.o(i + 1, j)] + um[g.o(i + 1, j - 1)]) * Ae / e;
-  double fw = 0.5 * (um[g.o(i, j)] + um[g.o(i, j - 1)]) * Aw / e;
-  double df = fe - fw + fn - fs;
-  double Dn = (e / d.Re) * An / (g.ym[j + 1] - g.ym[j]);
-  double Ds = (e / d.Re) * As / (g.ym[j] - g.ym[j - 1]);
-  double De = (e / d.Re) * Ae / (g.x[i + 1] - g.x[i]);
-  double Dw = (e / d.Re) * Aw / (g.x[i] - g.x[i - 1]);
-  double aw = Dw + pos(fw), as = Ds + pos(fs), ae = De + pos(-fe), an = Dn + pos(-fn);
-  double ap = aw + ae + as + an + df;
-  double vW = vm[g.o(i - 1, j)], vE = vm[g.o(i + 1, j)], vS = vm[g.o(i, j - 1)],
-         vN = vm[g.o(i, j + 1)], vP = vm[g.o(i, j)], uP = um[g.o(i, j)];
-  double q_art = e * (p[g.o(i, j)] - p[g.o(i, j - 1)]) / (g.y[j] - g.y[j - 1]);
-  if (d.flags & F_BART) {
-    double dvdydy = An * (vN - vP) / (g.ym[j + 1] - g.ym[j]) - As * (vP - vS) / (g.ym[j] - g.ym[j - 1]);
-    double dydudx = An * (um[g.o(i + 1, j)] - um[g.o(i, j)]) / (g.xm[i + 1] - g.xm[i]) -
-                    As * (um[g.o(i + 1, j - 1)] - um[g.o(i, j - 1)]) / (g.xm[i + 1] - g.xm[i]);
-    q_art = q_art - d.b_art * (dydudx + dvdydy);
-  }
-  double r = 1.0 / (g.x[i] - g.x[i - 1]) / (g.y[j] - g.y[j - 1]) *
-                 (-(ap * vP) + aw * vW + ae * vE + as * vS + an * vN) -
-             q_art;
-  if (d.flags & F_BUOY) r = r + buoyancy(d, g, T, i, j);
-  if (d.flags & F_POROUS)
-    r = r - e * (vP / (d.Re * d.Da) + d.Cf / sqrt(e * d.Da) * vP * sqrt(uP * uP + vP * vP)) * lg;
-  return r;
-}
-
-// ---- RESZ / RESC (equations.f90:738-759, 839-861) -------------------------------------------
-template <bool IS_C>
-__device__ double res_scalar(const CaseDev& d, const G& g, const double* un, const double* vn,
-                             const double* Z, int i, int j) {
-  const double k = IS_C ? 1.0 / d.Re / d.Sc : 1.0 / d.Pe;
-  double Zp = Z[g.o(i, j)], Ze = Z[g.o(i + 1, j)], Zw = Z[g.o(i - 1, j)], Zn = Z[g.o(i, j + 1)],
-         Zs = Z[g.o(i, j - 1)];
-  double Aew = g.ym[j + 1] - g.ym[j], Ans = g.xm[i + 1] - g.xm[i];
-  double dzu = 0.5 * (Ze + Zp) * un[g.o(i + 1, j)] * Aew - 0.5 * (Zw + Zp) * un[g.o(i, j)] * Aew;
-  double dzv = 0.5 * (Zn + Zp) * vn[g.o(i, j + 1)] * Ans - 0.5 * (Zs + Zp) * vn[g.o(i, j)] * Ans;
-  double De = (g.ym[j + 1] - g.ym[j]) * k / (g.x[i + 1] - g.x[i]);
-  double Dw = (g.ym[j + 1] - g.ym[j]) * k / (g.x[i] - g.x[i - 1]);
-  double Dn = (g.xm[i + 1] - g.xm[i]) * k / (g.y[j + 1] - g.y[j]);
-  double Ds = (g.xm[i + 1] - g.xm[i]) * k / (g.y[j] - g.y[j - 1]);
-  double Dp = De + Dw + Dn + Ds;
-  double lg = d.liga[g.o(i, j)], e = d.epsf[g.o(i, j)];
-  if (IS_C)
-    return 1.0 / (g.xm[i + 1] - g.xm[i]) / (g.ym[j + 1] - g.ym[j]) *
-           (-(Dp * Zp) + De * Ze + Dw * Zw + Dn * Zn + Ds * Zs - (dzu + dzv) / (lg * (e - 1.0) + 1.0));
-  return 1.0 / (g.xm[i + 1] - g.xm[i]) / (g.ym[j + 1] - g.ym[j]) *
-         (-(Dp * Zp) + De * Ze + Dw * Zw + Dn * Zn + Ds * Zs - (1.0 - lg) * (dzu + dzv)) /
-         (lg * (e - 1.0) + 1.0);
-}
-
-// Block-wide max of non-negative values, then one atomic per block.
-__device__ inline void block_max_to(unsigned long long* slot, double v) {
-  __shared__ double red[32];
-  unsigned m = 0xffffffffu;
-  for (int o = 16; o > 0; o >>= 1) {
-    double w = __shfl_xor_sync(m, v, o);
-    v = (w > v || w != w) ? w : v;
-  }
-  int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  int nw = (blockDim.x * blockDim.y + 31) / 32;
-  if ((tid & 31) == 0) red[tid >> 5] = v;
-  __syncthreads();
-  if (tid < 32) {
-    v = tid < nw ? red[tid] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) {
-      double w = __shfl_xor_sync(m, v, o);
-      v = (w > v || w != w) ? w : v;
-    }
-    if (tid == 0 && v != 0.0) atomic_max_nonneg(slot, v);
-  }
-}
-
-}  // namespace
+using namespace exact;
 
 // ---- solve_U stage s (s = 1,2,3; equations.f90:259-298) ---------------------------------------
 template <int STAGE>

@@ -1,4 +1,5 @@
 // kernels_fast.cu -- fused FAST-arithmetic kernels (placeholder until the fused path lands).
+#include "engine_api.h"
 #include "fast.h"
 
 namespace acs {
@@ -13,7 +14,10 @@ void fast_u(FastPlan*, const CaseDev*, CaseCtl*, const Tile*, int, int, cudaStre
 void fast_v(FastPlan*, const CaseDev*, CaseCtl*, const Tile*, int, int, cudaStream_t) {}
 void fast_p(FastPlan*, const CaseDev*, CaseCtl*, const Tile*, int, int, cudaStream_t) {}
 void fast_s(FastPlan*, bool, const CaseDev*, CaseCtl*, const Tile*, int, int, cudaStream_t) {}
+void fast_timed(FastPlan*, int, const CaseDev*, CaseCtl*, const Tile*, int, int, cudaStream_t) {}
 int fast_u_launches(const FastPlan*) { return 0; }
+cudaError_t launch_engine_fast(const EngineArgs&, int, int, cudaStream_t) { return cudaErrorNotSupported; }
+int max_active_clusters_fast(int) { return 0; }
 int fast_v_launches(const FastPlan*) { return 0; }
 int fast_p_launches(const FastPlan*) { return 0; }
 int fast_s_launches(const FastPlan*) { return 0; }

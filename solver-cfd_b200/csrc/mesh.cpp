@@ -138,4 +138,11 @@ double acs_noise(uint64_t seed, uint64_t case_id, uint64_t field, uint64_t index
   return amp * (2.0 * u - 1.0);
 }
 
+int acs_noise_array(uint64_t seed, uint64_t case_id, uint64_t field, const uint64_t* index, long long n,
+                    double amp, double* out) {
+  if (n < 0 || (n > 0 && (!index || !out))) return ACS_E_ARG;
+  for (long long k = 0; k < n; ++k) out[k] = acs_noise(seed, case_id, field, index[k], amp);
+  return ACS_OK;
+}
+
 }  // extern "C"

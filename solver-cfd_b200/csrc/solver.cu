@@ -20,6 +20,7 @@
 #include "../../include/acs.h"
 #include "acs_dev.cuh"
 #include "fast.h"
+#include "engine_api.h"
 #include "kernels.h"
 
 namespace acs {
@@ -95,6 +96,11 @@ struct Batch {
   long long launches = 0;
   long long body_kernels = 0;
   int graph_steps = -1;  // n_steps the graph's loop bound was built for
+  int engine = 0;        // 0 = persistent cluster engine, 1 = graph of per-stage kernels
+  int nodes_per_cta = 1536;
+  int* d_cases = nullptr;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> ev;
 
   ~Batch() {
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -104,6 +110,9 @@ struct Batch {
     if (d_iters) cudaFree(d_iters);
     if (d_err) cudaFree(d_err);
     if (h_flag) cudaFreeHost(h_flag);
+    if (d_cases) cudaFree(d_cases);
+    for (auto s : side) cudaStreamDestroy(s);
+    for (auto e : ev) cudaEventDestroy(e);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
 
@@ -203,6 +212,11 @@ bool all_ones(const double* a, size_t n) {
 int upload_field(Batch& b, int c, int field, const double* host) {
   FieldLoc L = field_loc(field);
   if (L.family < 0) return fail(ACS_E_ARG, "unknown field id");
+  if (field == ACS_UM_TAU || field == ACS_VM_TAU) {
+    b.hk[c].tau_dirty = 1;
+    int r = push_ctl(b);
+    if (r) return r;
+  }
   if (L.role == R_NTAU && L.family != 2 && b.hk[c].ntau_alias) {
     // give every n_tau array its own values again before one of them is overwritten
     CaseCtl& k = b.hk[c];
@@ -274,6 +288,7 @@ void reset_roles(CaseCtl& k) {
   k.rp[1] = 1;
   k.rp_read = 1;
   k.ntau_alias = 0;
+  k.tau_dirty = 1;
 }
 
 int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch** out) {
@@ -289,7 +304,7 @@ int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch**
     if ((params[c].arith == ACS_ARITH_FAST) != fast) return fail(ACS_E_ARG, "all cases of a batch must use one arith mode");
 
   // Layout of the pool: [case table][control][tiles][counters] then per case
-  // [metrics][eps][liga][mask][U x3][V x3][P x2][T x3][C x3][S x2].
+  // [metrics][eps][liga][mask][U x3][V x3][P x2][T x3][C x3][S x4].
   std::vector<size_t> off(n);
   std::vector<size_t> sizes(n);
   size_t total = 0;
@@ -297,7 +312,7 @@ int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch**
     const int nx = params[c].imax, ny = params[c].jmax;
     const size_t ne = align_up(nx + 1, 4) * (size_t)(ny + 1);
     size_t sz = align_up(sizeof(double) * (2 * nx + 2 * ny + 6), 256) + 2 * align_up(8 * ne, 256) +
-                align_up(ne, 256) + 16 * align_up(8 * ne, 256);
+                align_up(ne, 256) + 18 * align_up(8 * ne, 256);
     off[c] = total;
     sizes[c] = sz;
     total += align_up(sz, 256);
@@ -401,8 +416,7 @@ int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch**
         bufs[f][r] = (double*)q;
         q += align_up(8 * ne, 256);
       }
-    d.S[0] = (double*)q; q += align_up(8 * ne, 256);
-    d.S[1] = (double*)q; q += align_up(8 * ne, 256);
+    for (int r = 0; r < 4; ++r) { d.S[r] = (double*)q; q += align_up(8 * ne, 256); }
     reset_roles(b->hk[c]);
   }
   if (fast) {
@@ -461,6 +475,21 @@ void seq_s(Batch& b, bool is_c) {
     launch_bc_cell(b.dc, b.dk, b.n, w0 + s - 1, b.stream);
   }
   b.launches += 6;
+}
+
+// one launch of the timed kernel (acs_batch_time_kernel)
+void launch_timed_kernel(Batch& b, int kernel) {
+  if (b.use_fast) {
+    fast_timed(b.fast, kernel, b.dc, b.dk, b.dtiles, b.ntiles, b.n, b.stream);
+    return;
+  }
+  switch (kernel) {
+    case 0: launch_u_stage_exact(1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
+    case 1: launch_v_stage_exact(1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
+    case 2: launch_p_exact(b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
+    case 3: launch_s_stage_exact(false, 1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
+    case 4: launch_s_stage_exact(true, 1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
+  }
 }
 
 bool any_scalars(const Batch& b) {
@@ -542,6 +571,9 @@ int build_graph(Batch& b, int n_steps) {
   return ACS_OK;
 }
 
+int run_engine(Batch& b);
+int run_graph(Batch& b, int n_steps);
+
 int run_batch(Batch& b, int n_steps, int* itc, int* iters, double* err, int* status) {
   if (n_steps <= 0) return fail(ACS_E_ARG, "n_steps must be positive");
   int r = refresh_flags(b);
@@ -574,6 +606,34 @@ int run_batch(Batch& b, int n_steps, int* itc, int* iters, double* err, int* sta
   r = push_ctl(b);
   if (r) return r;
   CU(cudaMemsetAsync(b.d_nactive, 0, 256, b.stream));
+  if (b.engine == 0) {
+    r = run_engine(b);
+    if (r) return r;
+  } else {
+    r = run_graph(b, n_steps);
+    if (r) return r;
+  }
+  r = pull_ctl(b);
+  if (r) return r;
+  if (iters) CU(cudaMemcpy(iters, b.d_iters, sizeof(int) * need, cudaMemcpyDeviceToHost));
+  if (err) CU(cudaMemcpy(err, b.d_err, sizeof(double) * need, cudaMemcpyDeviceToHost));
+  bool failed = false;
+  for (int c = 0; c < b.n; ++c) {
+    if (itc) itc[c] = b.hk[c].itc;
+    if (status) status[c] = b.hk[c].status;
+    failed |= b.hk[c].status == ACS_CASE_FAILED;
+    b.hk[c].active = 0;
+  }
+  CU(cudaMemsetAsync(b.d_iter, 0, sizeof(long long), b.stream));
+  r = push_ctl(b);
+  if (r) return r;
+  CU(cudaStreamSynchronize(b.stream));
+  if (failed) return fail(ACS_E_STATE, "a case failed: NaN or infinite residual");
+  return ACS_OK;
+}
+
+int run_graph(Batch& b, int n_steps) {
+  int r;
   // the graph bakes in the loop bound; rebuild when n_steps changes the bound
   if (!b.gexec || b.graph_steps != n_steps) {
     r = build_graph(b, n_steps);
@@ -597,22 +657,71 @@ int run_batch(Batch& b, int n_steps, int* itc, int* iters, double* err, int* sta
   long long iters_done = 0;
   CU(cudaMemcpy(&iters_done, b.d_iter, sizeof(long long), cudaMemcpyDeviceToHost));
   b.launches = iters_done * b.body_kernels;
-  r = pull_ctl(b);
-  if (r) return r;
-  if (iters) CU(cudaMemcpy(iters, b.d_iters, sizeof(int) * need, cudaMemcpyDeviceToHost));
-  if (err) CU(cudaMemcpy(err, b.d_err, sizeof(double) * need, cudaMemcpyDeviceToHost));
-  bool failed = false;
-  for (int c = 0; c < b.n; ++c) {
-    if (itc) itc[c] = b.hk[c].itc;
-    if (status) status[c] = b.hk[c].status;
-    failed |= b.hk[c].status == ACS_CASE_FAILED;
-    b.hk[c].active = 0;
+  return ACS_OK;
+}
+
+// Cluster size for a case: about nodes_per_cta nodes per CTA, at most 16 CTAs, strips of at
+// least 4 node rows.
+int cluster_size(const Batch& b, int c) {
+  const CaseDev& d = b.hc[c];
+  const long long nodes = (long long)(d.nx + 1) * (d.ny + 1);
+  int K = (int)((nodes + b.nodes_per_cta - 1) / b.nodes_per_cta);
+  K = std::max(1, std::min(K, 16));
+  K = std::min(K, std::max(1, (d.ny + 1) / 4));
+  return K;
+}
+
+// One launch per cluster size, each on its own stream so the size classes run side by side.
+int run_engine(Batch& b) {
+  std::vector<std::vector<int>> groups(17);
+  for (int c = 0; c < b.n; ++c) groups[cluster_size(b, c)].push_back(c);
+  if (!b.d_cases) CU(cudaMalloc(&b.d_cases, sizeof(int) * b.n));
+  std::vector<int> order;
+  std::vector<std::pair<int, int>> launches;  // (K, offset)
+  for (int K = 16; K >= 1; --K) {
+    if (groups[K].empty()) continue;
+    launches.push_back({K, (int)order.size()});
+    order.insert(order.end(), groups[K].begin(), groups[K].end());
   }
-  CU(cudaMemsetAsync(b.d_iter, 0, sizeof(long long), b.stream));
-  r = push_ctl(b);
+  CU(cudaMemcpyAsync(b.d_cases, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice, b.stream));
+  for (int c = 0; c < b.n; ++c) {
+    std::memset(b.hk[c].slot, 0, sizeof(b.hk[c].slot));
+  }
+  int r = push_ctl(b);
   if (r) return r;
+  while (b.side.size() < launches.size()) {
+    cudaStream_t s;
+    CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    b.side.push_back(s);
+    cudaEvent_t e;
+    CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b.ev.push_back(e);
+  }
+  cudaEvent_t fork;
+  CU(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  CU(cudaEventRecord(fork, b.stream));
+  b.launches = 0;
+  for (size_t g = 0; g < launches.size(); ++g) {
+    const int K = launches[g].first;
+    const int off = launches[g].second;
+    const int cnt = (int)groups[K].size();
+    cudaStream_t s = g == 0 ? b.stream : b.side[g];
+    if (g) CU(cudaStreamWaitEvent(s, fork, 0));
+    EngineArgs a{b.dc, b.dk, b.d_cases + off, b.d_iters, b.d_err};
+    cudaError_t e = b.use_fast ? launch_engine_fast(a, K, cnt, s) : launch_engine_exact(a, K, cnt, s);
+    if (e != cudaSuccess) {
+      cudaEventDestroy(fork);
+      return fail(ACS_E_CUDA, std::string("engine launch (cluster ") + std::to_string(K) + "): " + cudaGetErrorString(e));
+    }
+    b.launches += 1;
+    if (g) {
+      CU(cudaEventRecord(b.ev[g], s));
+      CU(cudaStreamWaitEvent(b.stream, b.ev[g], 0));
+    }
+  }
+  cudaEventDestroy(fork);
   CU(cudaStreamSynchronize(b.stream));
-  if (failed) return fail(ACS_E_STATE, "a case failed: NaN or infinite residual");
+  CU(cudaGetLastError());
   return ACS_OK;
 }
 
@@ -646,6 +755,7 @@ double bits_to_double(unsigned long long v) {
 }  // namespace acs
 
 using acs::Batch;
+using acs::fail;
 
 struct acs_batch { Batch* b; };
 struct acs_handle { Batch* b; };
@@ -708,6 +818,73 @@ int acs_batch_get_field(acs_batch* h, int c, int field, double* host) {
 int acs_batch_run(acs_batch* h, int n_steps, int* itc, int* iters, double* err, int* status) {
   if (!h) return acs::fail(ACS_E_ARG, "null handle");
   return acs::run_batch(*h->b, n_steps, itc, iters, err, status);
+}
+
+int acs_batch_time_kernel(acs_batch* h, int kernel, int reps, double* ms_mean, long long* cells) {
+  if (!h || !ms_mean || reps <= 0 || kernel < 0 || kernel > 4) return acs::fail(ACS_E_ARG, "bad argument");
+  Batch& b = *h->b;
+  std::vector<acs::CaseCtl> saved = b.hk;
+  long long nc = 0;
+  for (int c = 0; c < b.n; ++c) {
+    b.hk[c].active = 1;
+    b.hk[c].scalars = 1;
+    const int nx = b.hc[c].nx, ny = b.hc[c].ny;
+    nc += kernel == 0 ? (long long)(nx - 3) * (ny - 2) : kernel == 1 ? (long long)(nx - 2) * (ny - 3)
+                                                                     : (long long)(nx - 2) * (ny - 2);
+  }
+  int r = acs::push_ctl(b);
+  if (r) return r;
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  auto one = [&]() { acs::launch_timed_kernel(b, kernel); };
+  if (kernel == 2)  // the pressure kernel writes pn: keep a copy in stage scratch
+    for (int c = 0; c < b.n; ++c)
+      CU(cudaMemcpyAsync(b.hc[c].S[1], b.hc[c].P[b.hk[c].rp[1]], 8 * b.hc[c].n_elems, cudaMemcpyDeviceToDevice, b.stream));
+  one();  // warm
+  CU(cudaEventRecord(e0, b.stream));
+  for (int i = 0; i < reps; ++i) one();
+  CU(cudaEventRecord(e1, b.stream));
+  CU(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CU(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CU(cudaGetLastError());
+  if (kernel == 2)
+    for (int c = 0; c < b.n; ++c)
+      CU(cudaMemcpyAsync(b.hc[c].P[b.hk[c].rp[1]], b.hc[c].S[1], 8 * b.hc[c].n_elems, cudaMemcpyDeviceToDevice, b.stream));
+  *ms_mean = ms / reps;
+  if (cells) *cells = nc;
+  for (int c = 0; c < b.n; ++c) {  // the residual slots were touched; restore the control words
+    saved[c].res_u = saved[c].res_v = saved[c].res_p = 0;
+  }
+  b.hk = saved;
+  r = acs::push_ctl(b);
+  if (!r) CU(cudaStreamSynchronize(b.stream));
+  return r;
+}
+
+int acs_batch_set_option(acs_batch* h, int option, long long value) {
+  if (!h) return acs::fail(ACS_E_ARG, "null handle");
+  Batch& b = *h->b;
+  switch (option) {
+    case ACS_OPT_ENGINE:
+      if (value != 0 && value != 1) return acs::fail(ACS_E_ARG, "engine must be 0 or 1");
+      b.engine = (int)value;
+      return ACS_OK;
+    case ACS_OPT_NODES_PER_CTA:
+      if (value < 64 || value > (1 << 22)) return acs::fail(ACS_E_ARG, "nodes per CTA out of range");
+      b.nodes_per_cta = (int)value;
+      return ACS_OK;
+  }
+  return acs::fail(ACS_E_ARG, "unknown option");
+}
+
+int acs_set_option(acs_handle* h, int option, long long value) {
+  if (!h) return acs::fail(ACS_E_ARG, "null handle");
+  acs_batch tmp{h->b};
+  return acs_batch_set_option(&tmp, option, value);
 }
 
 int acs_batch_launch_count(acs_batch* h, long long* n) {

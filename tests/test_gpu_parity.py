@@ -66,8 +66,14 @@ def test_routines_bit_exact(gpu, orc, which):
             assert np.array_equal(x, y), (name, k, float(np.nanmax(np.abs(x - y))))
 
 
-def _loop_compare(pkg, orc, prm, mesh, st, itc, nsteps):
+ENGINES = pytest.mark.parametrize("engine", [0, 1], ids=["cluster", "graph"])
+
+
+def _loop_compare(pkg, orc, prm, mesh, st, itc, nsteps, engine=0, nodes_per_cta=None):
     g = pkg.Case(prm, mesh)
+    g.set_option(pkg.OPT_ENGINE, engine)
+    if nodes_per_cta:
+        g.set_option(pkg.OPT_NODES_PER_CTA, nodes_per_cta)
     g.set_state(st)
     itc_g, it_g, er_g, status = g.physical_steps(nsteps, itc)
     out = g.get_state()
@@ -83,28 +89,42 @@ def _loop_compare(pkg, orc, prm, mesh, st, itc, nsteps):
     return it_g
 
 
-def test_loop_reference_small(gpu, orc):
+@ENGINES
+def test_loop_reference_small(gpu, orc, engine):
     prm, mesh, st, itc, _ = gpu.configs.reference_case(12, itc_max=5000)
-    it = _loop_compare(gpu, orc, prm, mesh, st, itc, 6)
+    it = _loop_compare(gpu, orc, prm, mesh, st, itc, 6, engine)
     assert it[0] >= 2
 
 
-def test_loop_channel_plain(gpu, orc):
+@ENGINES
+def test_loop_channel_plain(gpu, orc, engine):
     """cfg-plain shape (51 x 51, upwind, beta=1) with the pseudo loop capped at 1500 per step."""
     prm, mesh, st, itc, _ = gpu.configs.cfg_plain(itc_max=1500)
-    _loop_compare(gpu, orc, prm, mesh, st, itc, 2)
+    _loop_compare(gpu, orc, prm, mesh, st, itc, 2, engine)
 
 
-def test_loop_channel_full_physics(gpu, orc):
+@ENGINES
+def test_loop_channel_full_physics(gpu, orc, engine):
     """QUICK, porous block, buoyancy, both scalars; 2 steps of a 40 x 30 channel."""
     cfg = gpu.configs
     prm, mesh, st, itc = cfg.channel_case(40, 30, seed=3, Re=200.0, scheme=gpu.SCHEME_QUICK,
                                           block=cfg.centred_block(2, 1, 0.3), porosity=0.4, Da=1e-3,
                                           Cf=0.55, Ri=1.0, scalars=True, itc_max=1200)
-    _loop_compare(gpu, orc, prm, mesh, st, itc, 2)
+    _loop_compare(gpu, orc, prm, mesh, st, itc, 2, engine)
 
 
-def test_batch_equals_oracle_per_case(gpu, orc):
+@pytest.mark.parametrize("nodes_per_cta", [64, 300, 100000])
+def test_cluster_sizes_bit_exact(gpu, orc, nodes_per_cta):
+    """The engine's result does not depend on how a case is split into strips (1..16 CTAs)."""
+    cfg = gpu.configs
+    prm, mesh, st, itc = cfg.channel_case(37, 70, seed=5, Re=150.0, scheme=gpu.SCHEME_QUICK,
+                                          block=cfg.centred_block(2, 1, 0.3), porosity=0.5, Da=1e-2,
+                                          Cf=0.55, Ri=0.5, scalars=True, itc_max=500)
+    _loop_compare(gpu, orc, prm, mesh, st, itc, 2, 0, nodes_per_cta)
+
+
+@ENGINES
+def test_batch_equals_oracle_per_case(gpu, orc, engine):
     """Ragged batch (sizes, schemes, both boundary variants, converging and capped cases) in one
     graph launch; each case bit-identical to its own oracle run."""
     cfg = gpu.configs
@@ -119,6 +139,7 @@ def test_batch_equals_oracle_per_case(gpu, orc):
                                       porosity=q["porosity"], Da=q["Da"], Cf=0.55, Ri=q["Ri"],
                                       scalars=True, itc_max=700))
     b = gpu.Batch([x[0] for x in items], [x[1] for x in items])
+    b.set_option(gpu.OPT_ENGINE, engine)
     for c, x in enumerate(items):
         b.set_state(c, x[2])
     nsteps = 3

@@ -62,3 +62,23 @@ def test_channel_noise_only_on_update_region(pkg):
     assert (vm[:, :2] == 0).all() and (vm[0, :] == 0).all()
     assert 0 < np.abs(um).max() <= 1e-3 and 0 < np.abs(vm).max() <= 1e-3
     assert n == 200 and prm.beta == 1.0 and prm.eps == 1e-6 and prm.continuity == 1
+
+
+def test_noise_array_matches_scalar_and_oracle(pkg, orc):
+    import numpy as np
+    idx = np.array([0, 1, 5, 1000, 2**33 + 7], dtype=np.uint64)
+    a = pkg.noise_array(3, 9, 2, idx, 1e-3)
+    for k, i in enumerate(idx):
+        assert a[k] == pkg.noise(3, 9, 2, int(i), 1e-3) == orc.noise(3, 9, 2, int(i), 1e-3)
+
+
+def test_channel_noise_matches_oracle_generator(pkg, orc):
+    """The vectorised initial condition equals element-wise calls of the oracle's generator."""
+    prm, mesh, st, itc = pkg.configs.channel_case(13, 11, seed=4, case_id=2)
+    nx, ny = 13, 11
+    for j in range(2, ny):
+        for i in range(3, nx):
+            assert st["um"][i - 1, j - 1] == orc.noise(4, 2, 1, (i - 1) + (j - 1) * (nx + 1), 1e-3)
+    for j in range(3, ny):
+        for i in range(2, nx):
+            assert st["vm"][i - 1, j - 1] == orc.noise(4, 2, 2, (i - 1) + (j - 1) * nx, 1e-3)
