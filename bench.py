@@ -180,8 +180,18 @@ def run_product(args):
     dev = torch.device("cuda", torch.cuda.current_device())
     stream = torch.cuda.current_stream()
     items, kind = build_workload(pkg, args.workload, args.arith, seed_offset=rank, max_iters=args.max_iters)
+    tuned = None
+    from importlib import import_module
+    if args.launch_shape:
+        t, c_, n_ = (int(v) for v in args.launch_shape.split(","))
+        tuned = {"threads": t, "ctas_per_sm": c_, "nodes_per_cta": n_}
+    elif args.arith == "fast" and args.engine == "cluster":
+        tuned = import_module(pkg.__name__ + ".autotune").tune(pkg, items, use_cache=not args.retune)
     batch = pkg.Batch([x[0] for x in items], [x[1] for x in items])
     batch.set_stream(stream.cuda_stream)
+    batch.set_option(pkg.OPT_ENGINE, 0 if args.engine == "cluster" else 1)
+    if tuned:
+        import_module(pkg.__name__ + ".autotune").apply(batch, pkg, tuned)
     for c, x in enumerate(items):
         batch.set_state(c, x[2])
     itc = np.array([x[3] for x in items], np.int32)
@@ -192,6 +202,10 @@ def run_product(args):
     for w in range(args.warmup):
         itc, _, _, st = batch.run(1, itc)
     torch.cuda.synchronize()
+    # snapshot of the loop state at the start of the timed steps, so the end-to-end pass below
+    # replays exactly the same steps (same pseudo-iteration counts)
+    snap = [batch.get_state(c) for c in range(n_cases)]
+    itc_snap = itc.copy()
     if world > 1:
         dist.barrier()
     iters = np.zeros((n_cases, args.steps), np.int64)
@@ -221,21 +235,38 @@ def run_product(args):
                        "iterations": iters.tolist()}, f)
     value = steps_done * world / elapsed
 
-    # dominant kernel, timed alone
-    ms_u, nodes_u = batch.time_kernel(0, reps=50)
     peak, peak_kind = measured_peaks()
-    b_node = U_KERNEL_BYTES[args.arith]
-    achieved = b_node * nodes_u / (ms_u * 1e-3) / 1e9
     b_cu = BYTES_PER_CELL_UPDATE[kind]
     cell_updates = sum(iters[c].sum() * items[c][0].imax * items[c][0].jmax for c in range(n_cases))
     loop_gbs = b_cu * cell_updates / elapsed / 1e9
+    if args.engine == "cluster":
+        # the persistent engine kernel is the whole loop: one launch per size class and step
+        kern = "k_engine (persistent cluster engine, %s arithmetic)" % args.arith
+        achieved = loop_gbs
+        per_launch = {"bytes_per_cell_update": b_cu, "launches": launches,
+                      "cell_updates_per_launch": cell_updates / max(launches, 1),
+                      "ms_per_launch": elapsed * 1e3 / max(launches, 1)}
+    else:
+        ms_u, nodes_u = batch.time_kernel(0, reps=50)
+        b_node = U_KERNEL_BYTES[args.arith]
+        kern = "k_u_stage_exact (u-momentum stage, graph engine)"
+        achieved = b_node * nodes_u / (ms_u * 1e-3) / 1e9
+        per_launch = {"bytes_per_node": b_node, "nodes_per_launch": nodes_u, "ms_per_launch": ms_u}
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "engine_dram_bytes.json")
+    if args.engine == "cluster" and os.path.exists(tfile):
+        with open(tfile) as f:
+            bpcu = json.load(f).get(kind, {}).get("dram_bytes_per_cell_update")
+        if bpcu:
+            traffic = bpcu * cell_updates / max(launches, 1)
 
-    # end to end through the C ABI with host buffers (pinned)
-    e2e_steps = max(1, min(args.steps, 3))
+    # end to end through the C ABI with host buffers (pinned): the same steps as the timed region
+    e2e_steps = args.steps
+    itc = itc_snap.copy()
     host = []
     h2d = d2h = 0
     for c in range(n_cases):
-        got = batch.get_state(c)
+        got = snap[c]
         pinned = {}
         for n, a in got.items():
             t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
@@ -288,25 +319,24 @@ def run_product(args):
                 "cases_per_gpu": n_cases,
                 "cells_per_gpu": cells,
                 "arith": args.arith,
+                "engine": args.engine,
+                "launch_shape": tuned,
                 "pseudo_iterations_per_step_mean": total_iters / steps_done,
                 "steps_capped_at_itc_max": capped,
                 "l2": "flushed (256 MB write) before every timed step",
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             },
             "cell_updates_per_s": cell_updates * world / elapsed,
-            "roofline": {
+            "roofline": dict({
                 "bound": "hbm",
-                "kernel": "u-momentum " + ("stage" if args.arith == "exact" else "fused routine"),
+                "kernel": kern,
                 "achieved": achieved,
                 "peak": peak,
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst)" if peak_kind == "measured" else "fallback",
                 "unit": "GB/s",
                 "frac": achieved / peak,
-                "bytes_per_node": b_node,
-                "nodes_per_launch": nodes_u,
-                "ms_per_launch": ms_u,
-                "traffic": None,
-            },
+                "traffic": traffic,
+            }, **per_launch),
             "loop_roofline": {
                 "bytes_per_cell_update": b_cu,
                 "achieved": loop_gbs,
@@ -321,8 +351,6 @@ def run_product(args):
         if cpu is not None:
             line["cpu_baseline"] = {"value": cpu["steps_per_s"], "unit": "steps/s", "cores": cpu["cores"],
                                     "kind": "port", "sample": cpu["sample"]}
-        if args.traffic is not None:
-            line["roofline"]["traffic"] = args.traffic
         print(json.dumps(line))
     batch.close()
     if world > 1:
@@ -394,14 +422,17 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--workload", default="full-102", choices=sorted(WORKLOADS))
-    ap.add_argument("--arith", default="exact", choices=["exact", "fast"])
+    ap.add_argument("--arith", default="fast", choices=["exact", "fast"])
+    ap.add_argument("--engine", default="cluster", choices=["cluster", "graph"])
+    ap.add_argument("--retune", action="store_true", help="ignore the autotuner cache")
+    ap.add_argument("--launch-shape", default=None,
+                    help="threads,ctas_per_sm,nodes_per_cta: skip the autotuner (profiling runs)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of the timed kernel")
     ap.add_argument("--max-iters", type=int, default=None,
                     help="cap the pseudo-iterations of every physical step (profiling runs; the steps "
                          "are then not converged)")

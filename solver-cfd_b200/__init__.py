@@ -45,7 +45,7 @@ EXPORTED = (
     "acs_batch_run", "acs_batch_launch_count", "acs_launch_count", "acs_batch_time_kernel",
     "acs_batch_set_option", "acs_set_option",
 )
-OPT_ENGINE, OPT_NODES_PER_CTA = 1, 2
+OPT_ENGINE, OPT_NODES_PER_CTA, OPT_L1_LOADS, OPT_THREADS, OPT_CTAS_PER_SM = 1, 2, 3, 4, 5
 ENGINE_CLUSTER, ENGINE_GRAPH = 0, 1
 
 

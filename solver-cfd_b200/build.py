@@ -28,7 +28,8 @@ SOURCES = {
     "kernels_exact.cu": ["-fmad=false"],
     "engine_exact.cu": ["-fmad=false"],
     "control.cu": ["-fmad=false"],
-    "kernels_fast.cu": [],
+    "engine_fast.cu": [],
+    "fast_tables.cu": [],
     "solver.cu": [],
 }
 CXX_SOURCES = {"mesh.cpp": ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"]}

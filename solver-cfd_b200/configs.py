@@ -79,7 +79,7 @@ def stable_dtau(mesh, beta, dt, safety=0.85):
 
 def channel_case(nx, ny, *, seed=0, case_id=0, Re=100.0, scheme=SCHEME_QUICK, block=None,
                  block2=None, porosity=1.0, Da=1.0, Cf=0.0, Ri=0.0, Pr=0.7, Sc=1.0,
-                 scalars=False, beta=1.0, dt=1.0e-3, dtau=None, eps=1.0e-6, itc_max=100000,
+                 scalars=False, beta=1.0, dt=1.0e-3, dtau=None, eps=1.0e-6, itc_max=1000000,
                  noise_amp=1.0e-3, T_block=2.0, Lx=2.0, Ly=1.0, stretch=1.5, arith=ARITH_EXACT,
                  continuity=1):
     """Channel configuration.  Returns (params, mesh, state, itc0).  dtau=None picks

@@ -19,6 +19,9 @@ enum CaseFlags {
   F_BINARY = 8,    // epsilon1/liga take only (1,0) and (phi,1): fast path may use a byte mask
 };
 
+// per-case constants of the FAST arithmetic (CaseDev::fc)
+enum FastConst { FC_IPHI = 0, FC_IRE, FC_IREDA, FC_CFS, FC_IRESC, FC_IPE, FC_DTB, FC_N };
+
 struct CaseDev {
   int nx, ny, pitch, flags;
   int scheme, bc, solve_scalars, itc_max;
@@ -28,9 +31,11 @@ struct CaseDev {
   const double *x, *y, *xm, *ym;      // 1-based: x[1..nx], y[1..ny], xm[1..nx+1], ym[1..ny+1]
   const double *epsf, *liga;          // pitched cell fields
   const uint8_t* mask;                // pitched porous mask (1 = porous), F_BINARY only
-  // fast-path metric tables (1-based like x); see kernels_fast.cu
-  const double* mx;                   // per-i table, stride MX_STRIDE
-  const double* my;                   // per-j table, stride MY_STRIDE
+  // FAST arithmetic (engine_fast.cu): per-column / per-row metric tables of 4 doubles each,
+  // indexed like x and y, and per-case constants
+  const double* mx;
+  const double* my;
+  double fc[8];
   double* U[3];
   double* V[3];
   double* P[2];

@@ -33,7 +33,7 @@
 namespace acs {
 namespace cg = cooperative_groups;
 
-constexpr int ENGINE_THREADS = 256;
+constexpr int ENGINE_THREADS = 256;  // CTA width of the EXACT engine (the FAST engine also has 512)
 
 struct EngineArgs {
   const CaseDev* cs;
@@ -180,9 +180,10 @@ __device__ inline void block_max3(double a, double b, double c, unsigned long lo
 
 // ---- the engine --------------------------------------------------------------------------------
 // PT provides the per-node residuals: ru(d, uin, vt, pn, i, j), rv(d, ut, vin, pn, T, i, j),
-// rs<IS_C>(d, un, vn, z, i, j) and p_update(d, p0, un, vn, i, j, &r).
-template <class PT>
-__global__ void __launch_bounds__(ENGINE_THREADS, 1) k_engine(EngineArgs a) {
+// rs<IS_C>(d, un, vn, z, i, j), p_update(d, p0, un, vn, i, j, &r), and ld(ptr, q), the load used
+// for arrays that other CTAs of the cluster write.
+template <class PT, int NT, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) k_engine(EngineArgs a) {
   cg::cluster_group cl = cg::this_cluster();
   const int K = (int)cl.num_blocks();
   const int rank = (int)cl.block_rank();
@@ -222,11 +223,11 @@ __global__ void __launch_bounds__(ENGINE_THREADS, 1) k_engine(EngineArgs a) {
           for_nodes(s, 3, nx - 1, 2, ny - 1, [&](int i, int j) {
             const double RU = PT::ru(d, uin, vt, pn_read, i, j);
             const long long q = lin(i, j, d.pitch);
-            const double r = ((__ldcg(um + q) - __ldcg(utau + q)) + RU * d.dt) * d.dtau;
-            if (st == 1) uout[q] = __ldcg(utau + q) + r;
-            else if (st == 2) uout[q] = 0.75 * __ldcg(utau + q) + 0.25 * (__ldcg(uin + q) + r);
+            const double r = ((PT::ld(um, q) - PT::ld(utau, q)) + RU * d.dt) * d.dtau;
+            if (st == 1) uout[q] = PT::ld(utau, q) + r;
+            else if (st == 2) uout[q] = 0.75 * PT::ld(utau, q) + 0.25 * (PT::ld(uin, q) + r);
             else {
-              uout[q] = 1.0 / 3.0 * __ldcg(utau + q) + 2.0 / 3.0 * (__ldcg(uin + q) + r);
+              uout[q] = 1.0 / 3.0 * PT::ld(utau, q) + 2.0 / 3.0 * (PT::ld(uin, q) + r);
               const double ar = fabs(r);
               mu = (ar > mu || ar != ar) ? ar : mu;
             }
@@ -242,11 +243,11 @@ __global__ void __launch_bounds__(ENGINE_THREADS, 1) k_engine(EngineArgs a) {
           for_nodes(s, 2, nx - 1, 3, ny - 1, [&](int i, int j) {
             const double RV = PT::rv(d, ut, vin, pn_read, T, i, j);
             const long long q = lin(i, j, d.pitch);
-            const double r = ((__ldcg(vm + q) - __ldcg(vtau + q)) + RV * d.dt) * d.dtau;
-            if (st == 1) vout[q] = (__ldcg(vtau + q) + r);
-            else if (st == 2) vout[q] = (0.75 * __ldcg(vtau + q) + 0.25 * (__ldcg(vin + q) + r));
+            const double r = ((PT::ld(vm, q) - PT::ld(vtau, q)) + RV * d.dt) * d.dtau;
+            if (st == 1) vout[q] = (PT::ld(vtau, q) + r);
+            else if (st == 2) vout[q] = (0.75 * PT::ld(vtau, q) + 0.25 * (PT::ld(vin, q) + r));
             else {
-              vout[q] = 1.0 / 3.0 * __ldcg(vtau + q) + 2.0 / 3.0 * (__ldcg(vin + q) + r);
+              vout[q] = 1.0 / 3.0 * PT::ld(vtau, q) + 2.0 / 3.0 * (PT::ld(vin, q) + r);
               const double ar = fabs(r);
               mv = (ar > mv || ar != ar) ? ar : mv;
             }
@@ -296,10 +297,10 @@ __global__ void __launch_bounds__(ENGINE_THREADS, 1) k_engine(EngineArgs a) {
         for_nodes(s, 2, nx - 1, 2, ny - 1, [&](int i, int j) {
           const double Rz = isc ? PT::template rs<true>(d, un, vn, zin, i, j) : PT::template rs<false>(d, un, vn, zin, i, j);
           const long long q = lin(i, j, d.pitch);
-          const double r = ((__ldcg(z + q) - __ldcg(ztau + q)) + Rz * d.dt) * d.dtau;
-          if (st == 1) zout[q] = __ldcg(ztau + q) + r;
-          else if (st == 2) zout[q] = 0.75 * __ldcg(ztau + q) + 0.25 * (__ldcg(zin + q) + r);
-          else zout[q] = 1.0 / 3.0 * __ldcg(ztau + q) + 2.0 / 3.0 * (__ldcg(zin + q) + r);
+          const double r = ((PT::ld(z, q) - PT::ld(ztau, q)) + Rz * d.dt) * d.dtau;
+          if (st == 1) zout[q] = PT::ld(ztau, q) + r;
+          else if (st == 2) zout[q] = 0.75 * PT::ld(ztau, q) + 0.25 * (PT::ld(zin, q) + r);
+          else zout[q] = 1.0 / 3.0 * PT::ld(ztau, q) + 2.0 / 3.0 * (PT::ld(zin, q) + r);
         });
       }
       __syncthreads();
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(ENGINE_THREADS, 1) k_engine(EngineArgs a) {
         const double* src = f == 0 ? d.U[k.ru[R_TAU]] : f == 1 ? d.V[k.rv[R_TAU]] : f == 2 ? d.T[k.rt[R_TAU]] : d.C[k.rc[R_TAU]];
         double* dst = f == 0 ? d.U[k.ru[R_PHYS]] : f == 1 ? d.V[k.rv[R_PHYS]] : f == 2 ? d.T[k.rt[R_PHYS]] : d.C[k.rc[R_PHYS]];
         const long long q0 = lin(1, s.r0, d.pitch), q1 = lin(1, s.r1, d.pitch);
-        for (long long q = q0 + threadIdx.x; q < q1; q += blockDim.x) dst[q] = __ldcg(src + q);
+        for (long long q = q0 + threadIdx.x; q < q1; q += blockDim.x) dst[q] = PT::ld(src, q);
       }
       cl.sync();
     }

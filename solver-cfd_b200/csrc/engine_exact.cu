@@ -8,6 +8,7 @@
 namespace acs {
 
 struct PtExact {
+  static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldcg(a + q); }
   static __device__ __forceinline__ double ru(const CaseDev& d, const double* uin, const double* vt,
                                               const double* pn, int i, int j) {
     const exact::G g(d);
@@ -44,7 +45,7 @@ struct PtExact {
 };
 
 cudaError_t launch_engine_exact(const EngineArgs& a, int cluster, int nclusters, cudaStream_t s) {
-  auto kern = k_engine<PtExact>;
+  auto kern = k_engine<PtExact, ENGINE_THREADS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
@@ -62,7 +63,7 @@ cudaError_t launch_engine_exact(const EngineArgs& a, int cluster, int nclusters,
 }
 
 int max_active_clusters_exact(int cluster) {
-  auto kern = k_engine<PtExact>;
+  auto kern = k_engine<PtExact, ENGINE_THREADS>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cluster);

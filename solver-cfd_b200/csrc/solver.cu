@@ -98,6 +98,9 @@ struct Batch {
   int graph_steps = -1;  // n_steps the graph's loop bound was built for
   int engine = 0;        // 0 = persistent cluster engine, 1 = graph of per-stage kernels
   int nodes_per_cta = 1536;
+  int l1_loads = 1;      // FAST engine: load cluster-written arrays through L1
+  int threads = 512;     // FAST engine: threads per CTA (256 or 512)
+  int ctas_per_sm = 1;   // FAST engine with 256 threads: 1 or 2 resident CTAs per SM
   int* d_cases = nullptr;
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> ev;
@@ -440,7 +443,6 @@ int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch**
 // ---- launch sequences --------------------------------------------------------------------------
 // solve_U: three stages, each followed by bcUV(stage array, vm_tau) (equations.f90:259-296)
 void seq_u(Batch& b) {
-  if (b.use_fast) { fast_u(b.fast, b.dc, b.dk, b.dtiles, b.ntiles, b.n, b.stream); b.launches += fast_u_launches(b.fast); return; }
   for (int s = 1; s <= 3; ++s) {
     launch_u_stage_exact(s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
     launch_bc_uv(b.dc, b.dk, b.n, s - 1, b.stream);
@@ -450,7 +452,6 @@ void seq_u(Batch& b) {
 
 // solve_V: three stages, each followed by bcUV(um_tau, stage array) (equations.f90:561-598)
 void seq_v(Batch& b) {
-  if (b.use_fast) { fast_v(b.fast, b.dc, b.dk, b.dtiles, b.ntiles, b.n, b.stream); b.launches += fast_v_launches(b.fast); return; }
   for (int s = 1; s <= 3; ++s) {
     launch_v_stage_exact(s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
     launch_bc_uv(b.dc, b.dk, b.n, 3 + s - 1, b.stream);
@@ -460,7 +461,6 @@ void seq_v(Batch& b) {
 
 // solve_P: the stages fuse pointwise; the intermediate bcP(pi) never reaches the interior
 void seq_p(Batch& b) {
-  if (b.use_fast) { fast_p(b.fast, b.dc, b.dk, b.dtiles, b.ntiles, b.n, b.stream); b.launches += fast_p_launches(b.fast); return; }
   launch_p_exact(b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
   launch_bc_cell(b.dc, b.dk, b.n, 0, b.stream);
   b.launches += 2;
@@ -468,7 +468,6 @@ void seq_p(Batch& b) {
 
 // solve_Z / solve_C: three stages, each followed by bcZ / bcC
 void seq_s(Batch& b, bool is_c) {
-  if (b.use_fast) { fast_s(b.fast, is_c, b.dc, b.dk, b.dtiles, b.ntiles, b.n, b.stream); b.launches += fast_s_launches(b.fast); return; }
   const int w0 = is_c ? 4 : 1;
   for (int s = 1; s <= 3; ++s) {
     launch_s_stage_exact(is_c, s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
@@ -479,10 +478,6 @@ void seq_s(Batch& b, bool is_c) {
 
 // one launch of the timed kernel (acs_batch_time_kernel)
 void launch_timed_kernel(Batch& b, int kernel) {
-  if (b.use_fast) {
-    fast_timed(b.fast, kernel, b.dc, b.dk, b.dtiles, b.ntiles, b.n, b.stream);
-    return;
-  }
   switch (kernel) {
     case 0: launch_u_stage_exact(1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
     case 1: launch_v_stage_exact(1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
@@ -708,7 +703,8 @@ int run_engine(Batch& b) {
     cudaStream_t s = g == 0 ? b.stream : b.side[g];
     if (g) CU(cudaStreamWaitEvent(s, fork, 0));
     EngineArgs a{b.dc, b.dk, b.d_cases + off, b.d_iters, b.d_err};
-    cudaError_t e = b.use_fast ? launch_engine_fast(a, K, cnt, s) : launch_engine_exact(a, K, cnt, s);
+    cudaError_t e = b.use_fast ? launch_engine_fast(a, K, cnt, s, b.l1_loads, b.threads, b.ctas_per_sm)
+                               : launch_engine_exact(a, K, cnt, s);
     if (e != cudaSuccess) {
       cudaEventDestroy(fork);
       return fail(ACS_E_CUDA, std::string("engine launch (cluster ") + std::to_string(K) + "): " + cudaGetErrorString(e));
@@ -876,6 +872,17 @@ int acs_batch_set_option(acs_batch* h, int option, long long value) {
     case ACS_OPT_NODES_PER_CTA:
       if (value < 64 || value > (1 << 22)) return acs::fail(ACS_E_ARG, "nodes per CTA out of range");
       b.nodes_per_cta = (int)value;
+      return ACS_OK;
+    case ACS_OPT_L1_LOADS:
+      b.l1_loads = value ? 1 : 0;
+      return ACS_OK;
+    case ACS_OPT_THREADS:
+      if (value != 256 && value != 512) return acs::fail(ACS_E_ARG, "threads must be 256 or 512");
+      b.threads = (int)value;
+      return ACS_OK;
+    case ACS_OPT_CTAS_PER_SM:
+      if (value != 1 && value != 2) return acs::fail(ACS_E_ARG, "CTAs per SM must be 1 or 2");
+      b.ctas_per_sm = (int)value;
       return ACS_OK;
   }
   return acs::fail(ACS_E_ARG, "unknown option");

@@ -191,3 +191,42 @@ def test_reference_run_51x84_matches_golden(gpu):
         rel = np.abs(out[k] - ref[k]).max() / np.abs(ref[k]).max()
         assert rel < 1e-12, (k, rel)
     assert int(it_g.sum()) == 314712
+
+
+def _fast_compare(pkg, orc, prm, mesh, st, itc, nsteps, tol=1e-10, l1=0, nodes_per_cta=None):
+    from dataclasses import replace
+    g = pkg.Case(replace(prm, arith=pkg.ARITH_FAST), mesh)
+    g.set_option(pkg.OPT_L1_LOADS, l1)
+    if nodes_per_cta:
+        g.set_option(pkg.OPT_NODES_PER_CTA, nodes_per_cta)
+    g.set_state(st)
+    itc_g, it_g, er_g, status = g.physical_steps(nsteps, itc)
+    out = g.get_state()
+    ost = fcopy(st)
+    itc_o, it_o, er_o = orc.OracleCase(prm, mesh).run(ost, nsteps, itc)
+    assert status == pkg.CASE_DONE
+    assert list(it_g) == list(it_o), (list(it_g), list(it_o))
+    worst = 0.0
+    for k in ("um", "vm", "p", "T", "C", "um_tau", "vm_tau", "pn"):
+        x, y = mask_dead(k, out[k], prm.bc), mask_dead(k, ost[k], prm.bc)
+        rel = float(np.abs(x - y).max() / max(np.abs(y).max(), 1e-300))
+        worst = max(worst, rel)
+        assert rel < tol, (k, rel)
+    return worst
+
+
+@pytest.mark.parametrize("l1", [0, 1], ids=["l2-loads", "l1-loads"])
+def test_fast_engine_reference_case(gpu, orc, l1):
+    """FAST arithmetic, converged steps of the reference case: same pseudo-iteration count in
+    every step as the oracle and every field within 1e-10 relative max-norm."""
+    prm, mesh, st, itc, _ = gpu.configs.reference_case(12, itc_max=20000)
+    _fast_compare(gpu, orc, prm, mesh, st, itc, 8, l1=l1, nodes_per_cta=64)
+
+
+@pytest.mark.parametrize("l1", [0, 1], ids=["l2-loads", "l1-loads"])
+def test_fast_engine_channel_full_physics(gpu, orc, l1):
+    cfg = gpu.configs
+    prm, mesh, st, itc = cfg.channel_case(30, 22, seed=7, Re=120.0, scheme=gpu.SCHEME_QUICK,
+                                          block=cfg.centred_block(2, 1, 0.3), porosity=0.45, Da=1e-3,
+                                          Cf=0.55, Ri=1.0, scalars=True, eps=1e-5, itc_max=60000)
+    _fast_compare(gpu, orc, prm, mesh, st, itc, 3, l1=l1, nodes_per_cta=64)
