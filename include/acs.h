@@ -174,6 +174,24 @@ int acs_batch_run(acs_batch* b, int n_steps, int* itc, int* iters, double* err, 
  * nodes one launch updates. */
 int acs_batch_time_kernel(acs_batch* b, int kernel, int reps, double* ms_mean, long long* cells);
 
+/* ---- solve_U without device allocation --------------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc (their device memory
+ * belongs to another allocator, or they must not allocate once running): solve_U of
+ * acs_solve_u, with every array a DEVICE pointer in the Fortran layout (um, um_tau, um_n_tau:
+ * (imax+1) x jmax; vm_tau: imax x (jmax+1); pn and the grid's epsilon1/liga_poros: imax x jmax;
+ * the grid's x, y, xm, ym as in acs_grid) and no handle.  Its scratch is one static device array
+ * of ACS_STATIC_SCRATCH_BYTES that every GPU loading this library holds until exit; sizes beyond
+ * ACS_STATIC_MAX_DIM per direction or round_up(imax+1,4)*(jmax+1) > ACS_STATIC_MAX_NODES are
+ * rejected with ACS_E_SIZE.  The scratch address is looked up on the first call made on each
+ * device, so make that first call before any stream capture.  All calls share the scratch: calls
+ * that overlap on the GPU race.  The call synchronises `cuda_stream` (NULL = legacy default
+ * stream) and writes *residual_u on the host.  Arithmetic as ACS_ARITH_EXACT. */
+#define ACS_STATIC_MAX_DIM 4096
+#define ACS_STATIC_MAX_NODES 65536
+#define ACS_STATIC_SCRATCH_BYTES (5 * 1024 * 1024)
+int acs_solve_u_static(const acs_params* p, const acs_grid* grid_dev, const double* um, const double* um_tau,
+                       double* vm_tau, const double* pn, double* um_n_tau, double* residual_u, void* cuda_stream);
+
 /* Solver options (no reference counterpart). */
 enum acs_option {
   ACS_OPT_ENGINE = 1,        /* 0 (default): persistent cluster engine, one thread-block cluster

@@ -43,7 +43,7 @@ EXPORTED = (
     "acs_set_field", "acs_get_field", "acs_physical_steps", "acs_batch_create",
     "acs_batch_destroy", "acs_batch_set_stream", "acs_batch_set_field", "acs_batch_get_field",
     "acs_batch_run", "acs_batch_launch_count", "acs_launch_count", "acs_batch_time_kernel",
-    "acs_batch_set_option", "acs_set_option",
+    "acs_batch_set_option", "acs_set_option", "acs_solve_u_static",
 )
 OPT_ENGINE, OPT_NODES_PER_CTA, OPT_L1_LOADS, OPT_THREADS, OPT_CTAS_PER_SM = 1, 2, 3, 4, 5
 ENGINE_CLUSTER, ENGINE_GRAPH = 0, 1
@@ -123,6 +123,7 @@ def _declare(L):
     L.acs_batch_time_kernel.argtypes = [V, C.c_int, C.c_int, _D, C.POINTER(C.c_longlong)]
     L.acs_batch_set_option.argtypes = [V, C.c_int, C.c_longlong]
     L.acs_set_option.argtypes = [V, C.c_int, C.c_longlong]
+    L.acs_solve_u_static.argtypes = [C.POINTER(AcsParams), C.POINTER(AcsGrid), V, V, V, V, V, _D, V]
 
 
 def _check(code: int, where: str):

@@ -30,6 +30,7 @@ SOURCES = {
     "control.cu": ["-fmad=false"],
     "engine_fast.cu": [],
     "fast_tables.cu": [],
+    "noalloc.cu": [],
     "solver.cu": [],
 }
 CXX_SOURCES = {"mesh.cpp": ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"]}
