@@ -32,9 +32,11 @@ SOURCES = {
     "fast_tables.cu": [],
     "noalloc.cu": [],
     "solver.cu": [],
+    "../unet/csrc/unet_gemm.cu": [],
 }
 CXX_SOURCES = {"mesh.cpp": ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"]}
-HEADERS = ["acs_dev.cuh", "kernels.h", "fast.h", "engine.cuh", "engine_api.h", "points_exact.cuh"]
+HEADERS = [os.path.join(ROOT, "include", "unet.h"), "acs_dev.cuh", "kernels.h", "fast.h", "engine.cuh", "engine_api.h", "points_exact.cuh",
+           "../unet/csrc/gemm_tc.cuh"]
 
 
 def nvcc() -> str:
@@ -57,7 +59,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objs = []
     for src, extra in SOURCES.items():
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src + ".o")
+        o = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(o)
         if force or _newer(o, [s] + hdrs + [__file__]):
             cmd = [nvcc(), "-c", s, "-o", o] + NVCC_COMMON + extra

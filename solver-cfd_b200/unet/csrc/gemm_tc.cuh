@@ -1,0 +1,233 @@
+// gemm_tc.cuh -- BF16 x BF16 -> FP32 GEMM on the 5th-generation tensor cores (tcgen05).
+//
+//   D[m][n] = sum_k A[m][k] * B[n][k]        A: M x K, B: N x K, both row-major (K contiguous)
+//
+// One CTA (4 warps) computes a 128 x BN tile.  K is walked in slabs of 64: every slab of A and B
+// is copied to shared memory with 16-byte cp.async (zero fill outside the matrix) in the
+// canonical K-major, no-swizzle UMMA layout -- 8-row x 16-byte core matrices, the 8 K-chunks of
+// 16 bytes of a slab stored one after the other, each holding all rows -- so one shared-memory
+// descriptor per 16-wide K step addresses it (leading byte offset = distance between the two
+// K-chunks of a step, stride byte offset = 128 bytes between 8-row groups).  Thread 0 issues
+// tcgen05.mma.cta_group::1.kind::f16 (M = 128, N = BN, K = 16) with the accumulator in tensor
+// memory and commits to an mbarrier; slabs are double buffered so the copy of slab s+1 overlaps
+// the MMAs of slab s.  The epilogue reads the accumulator with tcgen05.ld (32 lanes x 32 bit,
+// 16 columns per load): warp w owns TMEM lanes 32w..32w+31, i.e. tile rows 32w..32w+31.
+//
+// Every wait on an mbarrier is bounded; on a timeout the kernel records the failure in *err,
+// frees its tensor memory and returns.
+#pragma once
+#include <cuda_bf16.h>
+#include <cstdint>
+
+namespace unet {
+
+constexpr int TC_BM = 128;
+constexpr int TC_BK = 64;
+constexpr int TC_THREADS = 128;
+constexpr long long TC_WAIT_LIMIT = 1ll << 26;
+
+enum Epilogue {
+  EPI_STORE_F32 = 0,   // C[m*ldc+n] = acc
+  EPI_ATOMIC_F32 = 1,  // C[m*ldc+n] += acc (split-K partial sums)
+  EPI_BIAS_BF16 = 2,   // Y[m*ldc+n] = bf16(act(acc + bias[n])), act = ReLU when relu != 0
+  EPI_BIAS_F32 = 3,    // C[m*ldc+n] = acc + bias[n]
+};
+
+struct GemmArgs {
+  const __nv_bfloat16* A;
+  const __nv_bfloat16* B;
+  int M, N, K;           // K: multiple of 8 (16-byte rows), lda/ldb in elements
+  int lda, ldb;
+  float* C;              // EPI_STORE_F32 / EPI_ATOMIC_F32 / EPI_BIAS_F32
+  __nv_bfloat16* Y;      // EPI_BIAS_BF16
+  int ldc;
+  const float* bias;
+  int relu;
+  int k_tiles_per_split; // split-K: blockIdx.z covers this many 64-wide K slabs
+  int* err;              // set to 1 when an mbarrier wait times out
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor (tcgen05): start address, leading/stride byte offsets (all >> 4),
+// version 1, base offset 0, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// Instruction descriptor, kind::f16: D F32, A and B BF16, both K-major, shape M x N.
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long long it = 0; it < TC_WAIT_LIMIT; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// Thread 0 waits (bounded) and the CTA learns the outcome together, so every thread takes the
+// same branch afterwards.
+__device__ __forceinline__ bool cta_wait(uint32_t bar, uint32_t parity, int* flag) {
+  if (threadIdx.x == 0) *flag = mbar_wait(bar, parity) ? 1 : 0;
+  __syncthreads();
+  return *flag != 0;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
+}
+
+// Copy one 64-wide K slab of `rows` rows starting at (r0, k0) into the UMMA layout at `sbase`.
+__device__ __forceinline__ void load_slab(uint32_t sbase, const __nv_bfloat16* G, int ld, int r0, int nrows_total,
+                                          int k0, int K, int rows) {
+  const int vecs = rows * (TC_BK / 8);
+  for (int v = threadIdx.x; v < vecs; v += TC_THREADS) {
+    const int r = v >> 3, c = v & 7;
+    const int gr = r0 + r, gk = k0 + c * 8;
+    const bool ok = gr < nrows_total && gk < K;
+    const __nv_bfloat16* src = ok ? G + (long long)gr * ld + gk : G;
+    cp_async16(sbase + (uint32_t)(c * rows * 16 + r * 16), src, ok);
+  }
+}
+
+template <int BN, int EPI>
+__global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(GemmArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  // layout: [2 stages][A: 128 x 64][B: BN x 64] bf16, then 2 mbarriers and the TMEM address
+  constexpr int A_BYTES = TC_BM * TC_BK * 2;
+  constexpr int B_BYTES = BN * TC_BK * 2;
+  constexpr int STAGE = A_BYTES + B_BYTES;
+  constexpr int TMEM_COLS = BN < 32 ? 32 : BN;
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + 2 * STAGE);
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(smem + 2 * STAGE + 16);
+  int* wait_flag = reinterpret_cast<int*>(smem + 2 * STAGE + 20);
+  const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * BN;
+  const int kt_total = (a.K + TC_BK - 1) / TC_BK;
+  const int kt0 = blockIdx.z * a.k_tiles_per_split;
+  const int kt1 = min(kt_total, kt0 + a.k_tiles_per_split);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(&bars[0]), 1);
+    mbar_init(smem_u32(&bars[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_holder;
+  constexpr uint32_t idesc = umma_idesc(TC_BM, BN);
+  bool ok = true;
+  uint32_t phase[2] = {0u, 0u};
+
+  for (int kt = kt0; kt < kt1; ++kt) {
+    const int s = (kt - kt0) & 1;
+    const uint32_t sa = smem_u32(smem + s * STAGE), sb = sa + A_BYTES;
+    if (kt - kt0 >= 2) {  // the MMAs that last read this stage must be done
+      ok = cta_wait(smem_u32(&bars[s]), phase[s], wait_flag);
+      phase[s] ^= 1u;
+      if (!ok) break;
+    }
+    load_slab(sa, a.A, a.lda, m0, a.M, kt * TC_BK, a.K, TC_BM);
+    load_slab(sb, a.B, a.ldb, n0, a.N, kt * TC_BK, a.K, BN);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+      for (int ks = 0; ks < TC_BK / 16; ++ks) {
+        const uint64_t da = umma_desc(sa + ks * 2 * TC_BM * 16, TC_BM * 16, 128);
+        const uint64_t db = umma_desc(sb + ks * 2 * BN * 16, BN * 16, 128);
+        const uint32_t acc = (kt > kt0 || ks > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+            ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   ::"r"(smem_u32(&bars[s])) : "memory");
+    }
+    __syncthreads();
+  }
+  // wait for the last commit of each stage still outstanding
+  const int nk = kt1 - kt0;
+  if (ok && nk > 0) {
+    for (int s = 0; s < 2; ++s) {
+      const int issued = nk > s ? (nk - s + 1) / 2 : 0;   // commits made on stage s
+      const int waited = nk > 2 + s ? (nk - 2 - s + 1) / 2 : 0;
+      if (issued > waited && ok) {
+        ok = cta_wait(smem_u32(&bars[s]), phase[s], wait_flag);
+        phase[s] ^= 1u;
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (!ok) {
+    if (threadIdx.x == 0 && a.err) atomicExch(a.err, 1);
+  } else if (nk > 0) {
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      uint32_t r[16];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < a.M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int n = n0 + c0 + j;
+          if (n >= a.N) break;
+          float v = __uint_as_float(r[j]);
+          const long long o = (long long)row * a.ldc + n;
+          if (EPI == EPI_STORE_F32) a.C[o] = v;
+          else if (EPI == EPI_ATOMIC_F32) atomicAdd(a.C + o, v);
+          else if (EPI == EPI_BIAS_F32) a.C[o] = v + (a.bias ? a.bias[n] : 0.f);
+          else {
+            v += a.bias ? a.bias[n] : 0.f;
+            if (a.relu) v = fmaxf(v, 0.f);
+            a.Y[o] = __float2bfloat16_rn(v);
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+}  // namespace unet
