@@ -205,6 +205,37 @@ enum acs_option {
 int acs_batch_set_option(acs_batch* b, int option, long long value);
 int acs_set_option(acs_handle* h, int option, long long value);
 
+/* ---- learned warm start (no counterpart in the reference) ------------------------------------
+ * Each case is drawn on a common H x W canvas (H >= jmax+1, W >= imax+1): node (i, j) of um, vm,
+ * p, T and C sits at pixel (j-1, i-1); pixels outside a field's shape are 0.  All tensors are
+ * DEVICE pointers, NHWC FP32, case-major, and ordered on the batch's stream.
+ *   acs_batch_ws_enable     allocates the per-case history (previous fields, last increment).
+ *   acs_batch_ws_features   updates the history (inc = fields - previous fields; 0 on the first
+ *                           call and after acs_batch_set_field), computes per case and field the
+ *                           RMS s of inc over the field's nodes (1 where inc is 0) and writes
+ *                           X[n][H][W][11] = u, v, p, T, C, porous indicator, inc_u/s_u, ...,
+ *                           inc_C/s_C.  inc_scale[n][8] (may be NULL) receives s.
+ *   acs_batch_ws_target     after a step: T[n][H][W][8] = (increment of this step - inc) / s
+ *                           (channels 0..4), Wt = 1 where the node exists, else 0.
+ *   acs_batch_set_start     start of the next pseudo-time loop.  Candidates: 0 plain (the stale
+ *                           pseudo-iterate the reference starts from), 1 extrapolated
+ *                           (fields + inc), 2 learned (fields + a[f] inc + s scale[f] Y[..][f]
+ *                           with a[f] = scale[8+f]; only when Y != NULL; scale has 16 entries),
+ *                           each with the boundary passes applied.
+ *                           policy 0 commits the candidate with the smallest initial residual
+ *                           (dtau-scaled max-norm of the U, V stage-1 and P updates); 1 the
+ *                           prediction (2 if Y, else 1); 2 plain.  chosen[n] (host, may be NULL)
+ *                           = the committed candidate; res0[3n] (host, may be NULL) = the three
+ *                           initial residuals (NaN for a candidate that was not built).
+ * The pseudo-time loop then iterates to the same tolerance from whichever start was kept. */
+#define ACS_WS_IN_CHANNELS 11
+#define ACS_WS_OUT_CHANNELS 8
+int acs_batch_ws_enable(acs_batch* b, int H, int W);
+int acs_batch_ws_features(acs_batch* b, float* X, float* inc_scale);
+int acs_batch_ws_target(acs_batch* b, float* T, float* Wt);
+int acs_batch_set_start(acs_batch* b, const float* Y, int ldy, const float* scale, int policy, int* chosen,
+                        double* res0);
+
 /* Number of kernel launches issued by the last acs_batch_run / acs_physical_steps. */
 int acs_batch_launch_count(acs_batch* b, long long* launches);
 int acs_launch_count(acs_handle* h, long long* launches);

@@ -20,6 +20,41 @@ extern "C" {
 int unet_gemm(const void* A, int lda, const void* B, int ldb, int M, int N, int K, int epilogue,
               float* C, void* Y, int ldc, const float* bias, int relu, int splits, int* err, void* stream);
 
+/* Layer kernels.  Activations are NHWC ([pixels][channels], pixels ordered batch, row, column).
+ * A 3x3 "same" convolution is the GEMM col(X) W^T with col(X)[m][(ky*3+kx)*C + c] =
+ * X[b][y+ky-1][x+kx-1][c] (zero outside the canvas and for k >= 9C; Kp = padded K, multiple of 8). */
+int unet_im2col(const void* X, int B, int H, int W, int C, int Kp, void* col, void* stream);
+/* dX[b][y][x][c] = sum over taps of dcol at the output pixels that read X[b][y][x][c] (FP32) */
+int unet_col2im(const float* dcol, int B, int H, int W, int C, int Kp, float* dX, void* stream);
+/* dst[c][r] = src[r][c] (BF16), r < rows, c < cols, row strides lds / ldd */
+int unet_transpose_bf16(const void* src, int rows, int cols, int lds, void* dst, int ldd, void* stream);
+/* 2x2 average pooling (H, W even), and its gradient (accumulate != 0 adds into dX) */
+int unet_pool_fwd(const void* X, int B, int H, int W, int C, void* Y, void* stream);
+int unet_pool_bwd(const float* dY, int B, int H, int W, int C, float* dX, int accumulate, void* stream);
+/* nearest 2x upsampling of X (B,h,w,C) into channels [cofs, cofs+C) of Y (B,2h,2w, row stride ldy),
+ * and its gradient (sum of the 4 children) */
+int unet_up_fwd(const void* X, int B, int h, int w, int C, void* Y, int ldy, int cofs, void* stream);
+int unet_up_bwd(const float* dY, int ldy, int cofs, int B, int h, int w, int C, float* dX, void* stream);
+/* channel-slice copies for the skip concatenations: Y[:, cofs:cofs+C] = X, dX (+)= dY[:, cofs:cofs+C] */
+int unet_copy_channels(const void* X, long long M, int C, void* Y, int ldy, int cofs, void* stream);
+int unet_take_channels(const float* dY, int ldy, int cofs, long long M, int C, float* dX, int accumulate,
+                       void* stream);
+/* dZ = bf16(relu ? dY * [Y > 0] : dY) over n values */
+int unet_act_bwd(const float* dY, const void* Y, long long n, int relu, void* dZ, void* stream);
+/* db[c] += sum_m dZ[m][c] (db must be zeroed by the caller) */
+int unet_bias_grad(const void* dZ, long long M, int C, float* db, void* stream);
+int unet_f32_to_bf16(const float* a, long long n, void* b, void* stream);
+/* *loss += sum w (out - tgt)^2 * inv_norm, dout = 2 w (out - tgt) inv_norm (loss zeroed by the caller) */
+int unet_mse(const float* out, const float* tgt, const float* w, long long n, float inv_norm, float* dout,
+             float* loss, void* stream);
+/* y = (x - shift[c]) * mul[c] over M pixels x C channels (FP32 in) to Y_bf16 and/or Y_f32 (either may be
+ * NULL, not both; Y_f32 may alias X) */
+int unet_normalize(const float* X, long long M, int C, const float* shift, const float* mul, void* Y_bf16,
+                   float* Y_f32, void* stream);
+/* Adam step t (>= 1) on FP32 master parameters p; p_bf16 (may be NULL) receives bf16(p) */
+int unet_adam(float* p, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
+              int t, void* p_bf16, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,7 +44,11 @@ EXPORTED = (
     "acs_batch_destroy", "acs_batch_set_stream", "acs_batch_set_field", "acs_batch_get_field",
     "acs_batch_run", "acs_batch_launch_count", "acs_launch_count", "acs_batch_time_kernel",
     "acs_batch_set_option", "acs_set_option", "acs_solve_u_static",
+    "acs_batch_ws_enable", "acs_batch_ws_features", "acs_batch_ws_target", "acs_batch_set_start",
 )
+WS_IN, WS_OUT = 11, 8
+POLICY_BEST, POLICY_PREDICTED, POLICY_PLAIN = 0, 1, 2
+START_PLAIN, START_EXTRAP, START_LEARNED = 0, 1, 2
 OPT_ENGINE, OPT_NODES_PER_CTA, OPT_L1_LOADS, OPT_THREADS, OPT_CTAS_PER_SM = 1, 2, 3, 4, 5
 ENGINE_CLUSTER, ENGINE_GRAPH = 0, 1
 
@@ -124,6 +128,10 @@ def _declare(L):
     L.acs_batch_set_option.argtypes = [V, C.c_int, C.c_longlong]
     L.acs_set_option.argtypes = [V, C.c_int, C.c_longlong]
     L.acs_solve_u_static.argtypes = [C.POINTER(AcsParams), C.POINTER(AcsGrid), V, V, V, V, V, _D, V]
+    L.acs_batch_ws_enable.argtypes = [V, C.c_int, C.c_int]
+    L.acs_batch_ws_features.argtypes = [V, V, V]
+    L.acs_batch_ws_target.argtypes = [V, V, V]
+    L.acs_batch_set_start.argtypes = [V, V, C.c_int, V, C.c_int, _I, _D]
 
 
 def _check(code: int, where: str):
@@ -405,6 +413,28 @@ class Batch:
         n = C.c_longlong(0)
         _check(lib().acs_batch_launch_count(self.h, C.byref(n)), "acs_batch_launch_count")
         return n.value
+
+    # ---- learned warm start (device pointers: torch tensors' data_ptr()) -------------------
+    def ws_enable(self, H: int, W: int):
+        _check(lib().acs_batch_ws_enable(self.h, H, W), "acs_batch_ws_enable")
+
+    def ws_features(self, X_ptr: int, scale_ptr: int = 0):
+        _check(lib().acs_batch_ws_features(self.h, C.c_void_p(X_ptr), C.c_void_p(scale_ptr or 0)),
+               "acs_batch_ws_features")
+
+    def ws_target(self, T_ptr: int, W_ptr: int):
+        _check(lib().acs_batch_ws_target(self.h, C.c_void_p(T_ptr), C.c_void_p(W_ptr)), "acs_batch_ws_target")
+
+    def set_start(self, Y_ptr, ldy: int, scale_ptr, policy: int):
+        """Choose the start of the next pseudo-time loop; returns (chosen[n], res0[n, 3]):
+        chosen = 0 plain, 1 extrapolated, 2 learned; res0 = the three initial residuals (NaN for
+        the learned one when Y_ptr is None)."""
+        chosen = np.zeros(self.n, np.int32)
+        res0 = np.zeros((self.n, 3))
+        _check(lib().acs_batch_set_start(self.h, C.c_void_p(Y_ptr or 0), ldy, C.c_void_p(scale_ptr or 0), policy,
+                                         chosen.ctypes.data_as(_I), res0.ctypes.data_as(_D)),
+               "acs_batch_set_start")
+        return chosen, res0
 
     def time_kernel(self, kernel: int, reps: int = 20):
         """Mean duration (ms) of one launch of a loop kernel and the nodes it updates."""

@@ -31,11 +31,13 @@ SOURCES = {
     "engine_fast.cu": [],
     "fast_tables.cu": [],
     "noalloc.cu": [],
+    "warmstart.cu": ["-fmad=false"],
     "solver.cu": [],
     "../unet/csrc/unet_gemm.cu": [],
+    "../unet/csrc/unet_ops.cu": [],
 }
 CXX_SOURCES = {"mesh.cpp": ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"]}
-HEADERS = [os.path.join(ROOT, "include", "unet.h"), "acs_dev.cuh", "kernels.h", "fast.h", "engine.cuh", "engine_api.h", "points_exact.cuh",
+HEADERS = [os.path.join(ROOT, "include", "unet.h"), "acs_dev.cuh", "kernels.h", "fast.h", "engine.cuh", "engine_api.h", "points_exact.cuh", "bc_exact.cuh", "warmstart.h",
            "../unet/csrc/gemm_tc.cuh"]
 
 

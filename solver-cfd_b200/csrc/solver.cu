@@ -22,6 +22,7 @@
 #include "fast.h"
 #include "engine_api.h"
 #include "kernels.h"
+#include "warmstart.h"
 
 namespace acs {
 
@@ -104,8 +105,23 @@ struct Batch {
   int* d_cases = nullptr;
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> ev;
+  // learned warm start (warmstart.cu): canvas size, per-case previous fields and increments
+  int ws_H = 0, ws_W = 0;
+  int ws_has_prev = 0;
+  char* ws_pool = nullptr;
+  WsCase* d_ws = nullptr;
+  unsigned long long* d_ws_res = nullptr;
+  int* d_ws_choice = nullptr;
+  double* d_ws_ss = nullptr;  // per case and field: sum of inc^2, then the RMS of inc
+  double* d_ws_sc = nullptr;
 
   ~Batch() {
+    if (ws_pool) cudaFree(ws_pool);
+    if (d_ws) cudaFree(d_ws);
+    if (d_ws_res) cudaFree(d_ws_res);
+    if (d_ws_choice) cudaFree(d_ws_choice);
+    if (d_ws_ss) cudaFree(d_ws_ss);
+    if (d_ws_sc) cudaFree(d_ws_sc);
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
     if (fast) fast_destroy(fast);
@@ -249,6 +265,7 @@ int upload_field(Batch& b, int c, int field, const double* host) {
     }
   }
   if (field == ACS_T) b.t_unity[c] = all_ones(host, (size_t)b.hc[c].nx * b.hc[c].ny);
+  b.ws_has_prev = 0;  // the increment history no longer describes the state
   return put(b, c, L.family, b.role_index(c, L), host);
 }
 
@@ -814,6 +831,82 @@ int acs_batch_get_field(acs_batch* h, int c, int field, double* host) {
 int acs_batch_run(acs_batch* h, int n_steps, int* itc, int* iters, double* err, int* status) {
   if (!h) return acs::fail(ACS_E_ARG, "null handle");
   return acs::run_batch(*h->b, n_steps, itc, iters, err, status);
+}
+
+int acs_batch_ws_enable(acs_batch* h, int H, int W) {
+  if (!h) return acs::fail(ACS_E_ARG, "null handle");
+  Batch& b = *h->b;
+  for (int c = 0; c < b.n; ++c)
+    if (b.hc[c].nx + 1 > W || b.hc[c].ny + 1 > H) return acs::fail(ACS_E_SIZE, "canvas smaller than (nx+1) x (ny+1)");
+  if (H <= 0 || W <= 0 || (long long)H * W > (1LL << 30)) return acs::fail(ACS_E_ARG, "bad canvas size");
+  if (!b.ws_pool) {
+    size_t bytes = 0;
+    for (int c = 0; c < b.n; ++c) bytes += 2 * acs::WS_FIELDS * acs::align_up(8 * b.hc[c].n_elems, 256);
+    CU(cudaMalloc(&b.ws_pool, bytes));
+    CU(cudaMemsetAsync(b.ws_pool, 0, bytes, b.stream));
+    std::vector<acs::WsCase> hw(b.n);
+    char* q = b.ws_pool;
+    for (int c = 0; c < b.n; ++c)
+      for (int f = 0; f < acs::WS_FIELDS; ++f) {
+        hw[c].prev[f] = (double*)q; q += acs::align_up(8 * b.hc[c].n_elems, 256);
+        hw[c].inc[f] = (double*)q; q += acs::align_up(8 * b.hc[c].n_elems, 256);
+      }
+    CU(cudaMalloc(&b.d_ws, sizeof(acs::WsCase) * b.n));
+    CU(cudaMemcpyAsync(b.d_ws, hw.data(), sizeof(acs::WsCase) * b.n, cudaMemcpyHostToDevice, b.stream));
+    CU(cudaMalloc(&b.d_ws_res, sizeof(unsigned long long) * 3 * b.n));
+    CU(cudaMalloc(&b.d_ws_choice, sizeof(int) * b.n));
+    CU(cudaMalloc(&b.d_ws_ss, sizeof(double) * acs::WS_OUT * b.n));
+    CU(cudaMalloc(&b.d_ws_sc, sizeof(double) * acs::WS_OUT * b.n));
+    CU(cudaMemsetAsync(b.d_ws_sc, 0, sizeof(double) * acs::WS_OUT * b.n, b.stream));
+    CU(cudaStreamSynchronize(b.stream));
+  }
+  b.ws_H = H;
+  b.ws_W = W;
+  b.ws_has_prev = 0;
+  return ACS_OK;
+}
+
+int acs_batch_ws_features(acs_batch* h, float* X, float* inc_scale) {
+  if (!h || !X) return acs::fail(ACS_E_ARG, "null argument");
+  Batch& b = *h->b;
+  if (!b.ws_pool) return acs::fail(ACS_E_STATE, "warm start not enabled");
+  acs::launch_ws_features(b.dc, b.dk, b.d_ws, b.n, b.ws_H, b.ws_W, b.ws_has_prev, b.d_ws_ss, b.d_ws_sc, X, inc_scale,
+                          b.stream);
+  CU(cudaGetLastError());
+  b.ws_has_prev = 1;
+  return ACS_OK;
+}
+
+int acs_batch_ws_target(acs_batch* h, float* T, float* Wt) {
+  if (!h || !T || !Wt) return acs::fail(ACS_E_ARG, "null argument");
+  Batch& b = *h->b;
+  if (!b.ws_pool) return acs::fail(ACS_E_STATE, "warm start not enabled");
+  acs::launch_ws_target(b.dc, b.dk, b.d_ws, b.n, b.ws_H, b.ws_W, b.d_ws_sc, T, Wt, b.stream);
+  CU(cudaGetLastError());
+  return ACS_OK;
+}
+
+int acs_batch_set_start(acs_batch* h, const float* Y, int ldy, const float* scale, int policy, int* chosen,
+                        double* res0) {
+  if (!h) return acs::fail(ACS_E_ARG, "null handle");
+  Batch& b = *h->b;
+  if (!b.ws_pool) return acs::fail(ACS_E_STATE, "warm start not enabled");
+  if (policy < 0 || policy > 2) return acs::fail(ACS_E_ARG, "policy must be 0, 1 or 2");
+  if (Y && (!scale || ldy < acs::WS_FIELDS)) return acs::fail(ACS_E_ARG, "Y needs scale and ldy >= 5");
+  acs::launch_ws_start(b.dc, b.dk, b.d_ws, b.n, b.ws_H, b.ws_W, b.d_ws_sc, Y, ldy, scale, policy, b.d_ws_res,
+                       b.d_ws_choice, b.stream);
+  CU(cudaGetLastError());
+  int r = acs::pull_ctl(b);  // the commit kernel set tau_dirty where the prediction was kept
+  if (r) return r;
+  if (chosen) CU(cudaMemcpy(chosen, b.d_ws_choice, sizeof(int) * b.n, cudaMemcpyDeviceToHost));
+  if (res0) {
+    std::vector<unsigned long long> bits(3 * b.n);
+    CU(cudaMemcpy(bits.data(), b.d_ws_res, sizeof(unsigned long long) * 3 * b.n, cudaMemcpyDeviceToHost));
+    for (int q = 0; q < 3 * b.n; ++q) res0[q] = acs::bits_to_double(bits[q]);
+    if (!Y)
+      for (int c = 0; c < b.n; ++c) res0[3 * c + 2] = std::nan("");
+  }
+  return ACS_OK;
 }
 
 int acs_batch_time_kernel(acs_batch* h, int kernel, int reps, double* ms_mean, long long* cells) {
