@@ -5,6 +5,12 @@ every case of the workload.  ``value`` is the whole-job throughput in converged 
 per second with the state resident in HBM; ``e2e`` is the same metric through the C ABI with the
 state copied from pinned host buffers before and back after every step.
 
+The default workload, ws-153, is the batched solver with the learned warm start: 16 held-out
+cases at 153 x 153 drawn from the batched configuration's parameter distribution, each step
+started from the best of the plain, extrapolated and learned start (the U-Net inference and the
+start selection are inside the timed region).  The plain GPU path is timed on the same steps
+from the same state and reported beside it (``plain_gpu``).
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--arith exact|fast]
     python bench.py --impl reference ...   # the CPU implementation of the loop on host cores
 
@@ -28,7 +34,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    # name: (description, bytes per cell-update of the fused model, config builder)
+    # name: description
+    "ws-153": "batched solver + learned warm start: 16 cases at 153 x 153, Re U[50,500], Da logU[1e-5,1e-2], "
+              "porosity U[0.3,0.9], Ri U[0,2], random block position (30% area), full equation set, QUICK, "
+              "residual 1e-6; cases seeded apart from the network's training cases",
     "full-102": "full equation set (u, v, p, T, C), QUICK, porous block 30% (porosity 0.4, Da 1e-3, Cf 0.55), "
                 "Ri 1, Pr 0.7, Sc 1, Re 200, 102 x 102 stretched 2:1 channel, beta 1, dt 1e-3, residual 1e-6",
     "full-204": "as full-102 on a 204 x 204 mesh",
@@ -53,6 +62,24 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """Max of a per-rank scalar over all ranks (the elapsed time of a step is the slowest rank's);
+    the identity on one rank."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed_offset(rank: int) -> int:
+    """Rank r runs its own replica of the workload with the seeds shifted by r (weak scaling:
+    the same case sizes and parameter distribution, different cases, no data exchange)."""
+    return rank
+
+
 def build_workload(pkg, name, arith, seed_offset=0, max_iters=None):
     items, kind = _build_workload(pkg, name, arith, seed_offset)
     if max_iters:
@@ -61,9 +88,15 @@ def build_workload(pkg, name, arith, seed_offset=0, max_iters=None):
     return items, kind
 
 
+WS_CASES, WS_N, WS_SEED = 16, 153, 101   # held-out seed (the network trains on seed 100)
+
+
 def _build_workload(pkg, name, arith, seed_offset=0):
     cfg = pkg.configs
     a = pkg.ARITH_FAST if arith == "fast" else pkg.ARITH_EXACT
+    if name == "ws-153":
+        items, _ = cfg.cfg_batch(WS_CASES, seed=WS_SEED + 1000 * seed_offset, sizes=(WS_N,), arith=a)
+        return items, "full"
     if name == "batch-256":
         items, _ = cfg.cfg_batch(256, seed=seed_offset, arith=a)
         return items, "full"
@@ -179,7 +212,10 @@ def run_product(args):
         raise SystemExit("no CUDA device")
     dev = torch.device("cuda", torch.cuda.current_device())
     stream = torch.cuda.current_stream()
-    items, kind = build_workload(pkg, args.workload, args.arith, seed_offset=rank, max_iters=args.max_iters)
+    items, kind = build_workload(pkg, args.workload, args.arith, seed_offset=replica_seed_offset(rank),
+                                 max_iters=args.max_iters)
+    if args.workload.startswith("ws-"):
+        return run_ws(args, pkg, items, kind, world, rank, dev, stream)
     tuned = None
     from importlib import import_module
     if args.launch_shape:
@@ -221,11 +257,7 @@ def run_product(args):
             launches += batch.launch_count()
         t_ev1.record(stream)
         torch.cuda.synchronize()
-    elapsed = t_ev0.elapsed_time(t_ev1) / 1e3
-    if world > 1:
-        t = torch.tensor([elapsed], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(t_ev0.elapsed_time(t_ev1) / 1e3, world, dev)
     total_iters = int(iters.sum())
     steps_done = n_cases * args.steps
     capped = int(sum((iters[c] >= items[c][0].itc_max - 1).sum() for c in range(n_cases)))
@@ -285,11 +317,7 @@ def run_product(args):
         for c in range(n_cases):
             batch.get_state(c, out={n: v for n, (t, v) in host[c].items()})
     torch.cuda.synchronize()
-    e2e_elapsed = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_elapsed], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_elapsed = float(t.item())
+    e2e_elapsed = max_over_ranks(time.perf_counter() - t0, world, dev)
     e2e = n_cases * e2e_steps * world / e2e_elapsed
 
     cpu = None
@@ -353,6 +381,271 @@ def run_product(args):
                                     "kind": "port", "sample": cpu["sample"]}
         print(json.dumps(line))
     batch.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def _tuned_batch(pkg, items, args, stream):
+    from importlib import import_module
+    tuned = None
+    if args.launch_shape:
+        t, c_, n_ = (int(v) for v in args.launch_shape.split(","))
+        tuned = {"threads": t, "ctas_per_sm": c_, "nodes_per_cta": n_}
+    elif args.arith == "fast" and args.engine == "cluster":
+        tuned = import_module(pkg.__name__ + ".autotune").tune(pkg, items, use_cache=not args.retune)
+
+    def make(states=None):
+        b = pkg.Batch([x[0] for x in items], [x[1] for x in items])
+        b.set_stream(stream.cuda_stream)
+        b.set_option(pkg.OPT_ENGINE, 0 if args.engine == "cluster" else 1)
+        if tuned:
+            import_module(pkg.__name__ + ".autotune").apply(b, pkg, tuned)
+        for c, x in enumerate(items):
+            b.set_state(c, states[c] if states is not None else x[2])
+        return b
+    return make, tuned
+
+
+def run_ws(args, pkg, items, kind, world, rank, dev, stream):
+    """Batched solver with the learned warm start (ws-* workloads)."""
+    import numpy as np
+    import torch
+    from importlib import import_module
+    ws = import_module(pkg.__name__ + ".warmstart")
+    unet = import_module(pkg.__name__ + ".unet")
+    if world > 1:
+        import torch.distributed as dist
+    net, norm, H, W, meta = ws.load(args.weights)
+    n_cases = len(items)
+    make, tuned = _tuned_batch(pkg, items, args, stream)
+    l2 = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+
+    A = make()
+    wA = ws.WarmStart(A, H, W, net, norm)
+    itc = np.array([x[3] for x in items], np.int32)
+    prev_snap = None
+    for w in range(args.warmup):
+        if w == args.warmup - 1:
+            prev_snap = [A.get_state(c) for c in range(n_cases)]
+        itc, _, _, _ = wA.step(itc, "learned")
+    torch.cuda.synchronize()
+    snap = [A.get_state(c) for c in range(n_cases)]
+    itc_snap = itc.copy()
+
+    def timed(step_fn, batch, itc):
+        """K steps; returns (elapsed s, iterations [n, K], chosen starts [n, K], engine ms, start ms,
+        launches)."""
+        iters = np.zeros((n_cases, args.steps), np.int64)
+        chosen = np.zeros((n_cases, args.steps), np.int64)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        eng_ms = 0.0
+        launches = 0
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for k in range(args.steps):
+            l2.fill_(float(k))
+            itc, it, ch, ms = step_fn(batch, itc)
+            iters[:, k] = it
+            chosen[:, k] = ch
+            eng_ms += ms
+            launches += batch.launch_count()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        el = max_over_ranks(ev[0].elapsed_time(ev[1]) / 1e3, world, dev)
+        return el, iters, chosen, eng_ms, launches, itc
+
+    def ws_step(batch, itc, w=wA):
+        w.features()
+        y = w.predict()
+        chosen, _ = batch.set_start(y.data_ptr(), 8, w.norm.out_scale.data_ptr(), pkg.POLICY_BEST)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        itc, it, _, _ = batch.run(1, itc)
+        e1.record(stream)
+        e1.synchronize()
+        return itc, it[:, 0], chosen, e0.elapsed_time(e1)
+
+    def plain_step(batch, itc):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        itc, it, _, _ = batch.run(1, itc)
+        e1.record(stream)
+        e1.synchronize()
+        return itc, it[:, 0], np.zeros(n_cases, np.int64), e0.elapsed_time(e1)
+
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        el_ws, it_ws, ch_ws, eng_ms, launches, _ = timed(ws_step, A, itc_snap.copy())
+    A.close()
+    # network inference alone, timed on the same canvas (FLOPs of the 15 convolutions)
+    x_in = net.input_buffer(n_cases, H, W)
+    for _ in range(2):
+        net.forward(n_cases, H, W)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    reps = 5
+    for _ in range(reps):
+        net.forward(n_cases, H, W)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / reps
+    fwd_flops = unet.conv_flops(H, W) * n_cases
+    del x_in
+
+    # plain GPU path, same steps from the same state
+    B = make(snap)
+    el_pl, it_pl, _, eng_pl, _, _ = timed(plain_step, B, itc_snap.copy())
+    plain_state = [B.get_state(c, ("um", "vm", "pn", "T", "C")) for c in range(n_cases)]
+    B.close()
+
+    # end to end through the C ABI with pinned host buffers: the same steps again
+    C_ = make(prev_snap)
+    wC = ws.WarmStart(C_, H, W, net, norm)
+    wC.features()                       # history: the fields at the start of the last warm-up step
+    host = []
+    h2d = d2h = 0
+    for c in range(n_cases):
+        pinned = {}
+        for nme, a in snap[c].items():
+            t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+            v = t.numpy().reshape(a.shape, order="F")
+            v[...] = a
+            pinned[nme] = (t, v)
+            h2d += a.nbytes
+            d2h += a.nbytes
+        host.append(pinned)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    itc = itc_snap.copy()
+    it_e2e = np.zeros((n_cases, args.steps), np.int64)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        for c in range(n_cases):
+            C_.set_state(c, {nme: v for nme, (t, v) in host[c].items()})
+        itc, it, _, _ = ws_step(C_, itc, wC)
+        it_e2e[:, k] = it
+        for c in range(n_cases):
+            C_.get_state(c, out={nme: v for nme, (t, v) in host[c].items()})
+    torch.cuda.synchronize()
+    e2e_el = time.perf_counter() - t0
+    ws_state = [{k: host[c][k][1] for k in ("um", "vm", "pn", "T", "C")} for c in range(n_cases)]
+    C_.close()
+    e2e_el = max_over_ranks(e2e_el, world, dev)
+    err = {}
+    for c in range(n_cases):
+        for k, v in ws.field_error(ws_state[c], plain_state[c]).items():
+            err[k] = max(err.get(k, 0.0), v)
+
+    # kernels of the warm start per step: history, scale, features; input normalisation; the
+    # network (im2col + GEMM per convolution, pool/upsample/skip copy per level); candidates,
+    # boundary passes, residual probes, commit
+    n_unet = 2 * len(net.convs) + 3 * (net.levels - 1)
+    ws_launches = args.steps * (3 + 1 + n_unet + 8)
+    steps_done = n_cases * args.steps
+    value = steps_done * world / el_ws
+    plain_value = steps_done * world / el_pl
+    peak, peak_kind = measured_peaks()
+    b_cu = BYTES_PER_CELL_UPDATE[kind]
+    cells = items[0][0].imax * items[0][0].jmax
+    cu_ws = int(it_ws.sum()) * cells
+    cu_pl = int(it_pl.sum()) * cells
+    eng_gbs = b_cu * cu_ws / (eng_ms * 1e-3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "engine_dram_bytes.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            bpcu = json.load(f).get(kind, {}).get("dram_bytes_per_cell_update")
+        if bpcu:
+            traffic = bpcu * cu_ws / max(launches, 1)
+    bf16_peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            bf16_peak = float(json.load(f)["bf16_tflops"])
+    except (OSError, KeyError, ValueError):
+        bf16_peak = 1590.0
+    if args.record_iterations and rank == 0:
+        rec = {}
+        if os.path.exists(args.record_iterations):
+            with open(args.record_iterations) as f:
+                rec = json.load(f)
+        rec[args.workload] = {"warmup": args.warmup, "steps": args.steps,
+                              "plain_iterations": it_pl.tolist(),
+                              "mean_iterations_per_step": [float(v) for v in it_pl.mean(axis=1)],
+                              "warm_start_iterations": it_ws.tolist()}
+        with open(args.record_iterations, "w") as f:
+            json.dump(rec, f, indent=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as orc
+        gips = [float(it_pl[c].mean()) for c in range(n_cases)]
+        state_items = [(x[0], x[1], snap[c], 0) for c, x in enumerate(items)]
+        cpu = cpu_sample(orc, state_items, gips, budget_s=args.cpu_seconds)
+    if rank == 0:
+        starts = np.bincount(ch_ws.ravel(), minlength=3) / ch_ws.size
+        line = {
+            "metric": "converged physical steps/s at pseudo-time residual 1e-6",
+            "value": value,
+            "unit": "steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": el_ws / args.steps * 1e3,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded channel cases; no public dataset)",
+            "config": {
+                "workload": args.workload,
+                "description": WORKLOADS[args.workload],
+                "cases_per_gpu": n_cases,
+                "cells_per_gpu": cells * n_cases,
+                "arith": args.arith,
+                "engine": args.engine,
+                "launch_shape": tuned,
+                "network": {"weights": os.path.relpath(args.weights, ROOT), "canvas": [H, W],
+                            "trained_snapshots": meta.get("snapshots")},
+                "pseudo_iterations_per_step_mean": float(it_ws.mean()),
+                "starts_plain_extrap_learned": starts.round(3).tolist(),
+                "l2": "flushed (256 MB write) before every timed step",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            },
+            "plain_gpu": {"value": plain_value, "unit": "steps/s", "ms_per_step": el_pl / args.steps * 1e3,
+                          "pseudo_iterations_per_step_mean": float(it_pl.mean()),
+                          "speedup_of_warm_start": value / plain_value,
+                          "final_fields_max_rel_diff_warm_vs_plain": err},
+            "cell_updates_per_s": cu_ws * world / el_ws,
+            "roofline": {
+                "bound": "hbm",
+                "kernel": "k_engine (persistent cluster engine, %s arithmetic)" % args.arith,
+                "achieved": eng_gbs,
+                "peak": peak,
+                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst)" if peak_kind == "measured" else "fallback",
+                "unit": "GB/s",
+                "frac": eng_gbs / peak,
+                "traffic": traffic,
+                "bytes_per_cell_update": b_cu,
+                "launches": launches,
+                "ms_per_launch": eng_ms / max(launches, 1),
+                "engine_share_of_step": eng_ms * 1e-3 / el_ws,
+            },
+            "unet_inference": {"bound": "tensor", "flops_per_launch_set": fwd_flops, "ms": fwd_ms,
+                               "achieved_tflops": fwd_flops / (fwd_ms * 1e-3) / 1e12,
+                               "peak_tflops": bf16_peak, "frac": fwd_flops / (fwd_ms * 1e-3) / 1e12 / bf16_peak},
+            "e2e": {"value": n_cases * args.steps * world / e2e_el, "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": args.steps,
+                    "same_iterations_as_timed": bool((it_e2e == it_ws).all())},
+            "gpu_launches": launches + ws_launches,
+            "gpu_launches_detail": {"engine": launches, "warm_start_and_network": ws_launches},
+            "clocks": clk.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = {"value": cpu["steps_per_s"], "unit": "steps/s", "cores": cpu["cores"],
+                                    "kind": "port", "sample": cpu["sample"] + " (plain start's iteration counts)"}
+        print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -422,10 +715,12 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
-    ap.add_argument("--workload", default="full-102", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="ws-153", choices=sorted(WORKLOADS))
+    ap.add_argument("--weights", default=os.path.join(ROOT, "solver-cfd_b200", "unet", "weights", "ws_153.npz"),
+                    help="trained warm-start network (ws-* workloads)")
     ap.add_argument("--arith", default="fast", choices=["exact", "fast"])
     ap.add_argument("--engine", default="cluster", choices=["cluster", "graph"])
     ap.add_argument("--retune", action="store_true", help="ignore the autotuner cache")

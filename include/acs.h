@@ -211,7 +211,8 @@ int acs_set_option(acs_handle* h, int option, long long value);
  * DEVICE pointers, NHWC FP32, case-major, and ordered on the batch's stream.
  *   acs_batch_ws_enable     allocates the per-case history (previous fields, last increment).
  *   acs_batch_ws_features   updates the history (inc = fields - previous fields; 0 on the first
- *                           call and after acs_batch_set_field), computes per case and field the
+ *                           call after acs_batch_ws_enable; fields uploaded in between count as
+ *                           the new fields), computes per case and field the
  *                           RMS s of inc over the field's nodes (1 where inc is 0) and writes
  *                           X[n][H][W][11] = u, v, p, T, C, porous indicator, inc_u/s_u, ...,
  *                           inc_C/s_C.  inc_scale[n][8] (may be NULL) receives s.

@@ -265,7 +265,6 @@ int upload_field(Batch& b, int c, int field, const double* host) {
     }
   }
   if (field == ACS_T) b.t_unity[c] = all_ones(host, (size_t)b.hc[c].nx * b.hc[c].ny);
-  b.ws_has_prev = 0;  // the increment history no longer describes the state
   return put(b, c, L.family, b.role_index(c, L), host);
 }
 

@@ -223,7 +223,7 @@ def train(net: UNet, X, T, Wt, H, W, norm: Normalizer, epochs=10, batch=16, lr=1
             k += 1
         m = float(acc.item()) / max(1, nb)
         losses.append(m)
-        if log:
+        if log and (ep % max(1, epochs // 20) == 0 or ep == epochs - 1):
             log(f"epoch {ep}: loss {m:.4e}")
     if net.wait_error():
         raise RuntimeError("a GEMM wait timed out during training")
