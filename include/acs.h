@@ -200,7 +200,10 @@ enum acs_option {
   ACS_OPT_NODES_PER_CTA = 2, /* engine: target nodes per CTA when sizing a case's cluster */
   ACS_OPT_L1_LOADS = 3,      /* FAST engine: 1 (default) reads cluster-written arrays through L1 */
   ACS_OPT_THREADS = 4,       /* FAST engine: threads per CTA, 256 or 512 (default) */
-  ACS_OPT_CTAS_PER_SM = 5    /* FAST engine, 256 threads: 2 caps registers so two CTAs share an SM */
+  ACS_OPT_CTAS_PER_SM = 5,   /* FAST engine, 256 threads: 2 caps registers so two CTAs share an SM */
+  ACS_OPT_STAGED = 6         /* FAST engine: 1 (default) copies each phase's stencil arrays (the
+                                CTA's rows plus two halo rows) into shared memory first, where
+                                they fit in 220 KB; 0 reads them from L1/L2 */
 };
 int acs_batch_set_option(acs_batch* b, int option, long long value);
 int acs_set_option(acs_handle* h, int option, long long value);

@@ -49,7 +49,7 @@ EXPORTED = (
 WS_IN, WS_OUT = 11, 8
 POLICY_BEST, POLICY_PREDICTED, POLICY_PLAIN = 0, 1, 2
 START_PLAIN, START_EXTRAP, START_LEARNED = 0, 1, 2
-OPT_ENGINE, OPT_NODES_PER_CTA, OPT_L1_LOADS, OPT_THREADS, OPT_CTAS_PER_SM = 1, 2, 3, 4, 5
+OPT_ENGINE, OPT_NODES_PER_CTA, OPT_L1_LOADS, OPT_THREADS, OPT_CTAS_PER_SM, OPT_STAGED = 1, 2, 3, 4, 5, 6
 ENGINE_CLUSTER, ENGINE_GRAPH = 0, 1
 
 

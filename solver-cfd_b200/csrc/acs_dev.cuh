@@ -42,6 +42,8 @@ struct CaseDev {
   double* T[3];
   double* C[3];
   double* S[4];                       // stage scratch (largest field shape)
+  double* S2[4];                      // stage scratch of T and C in the persistent engine, where
+                                      // their stages overlap the next iteration's U and V stages
   long long n_elems;                  // pitch * (ny+1): doubles per buffer
 };
 

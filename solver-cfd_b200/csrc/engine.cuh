@@ -10,10 +10,11 @@
 // Schedule of one pseudo-iteration (the reference runs solve_U, solve_V, solve_P, solve_Z,
 // solve_C one after the other; V reads um_tau, not um_n_tau, so U and V are independent, and
 // P, Z, C all read the new velocities only):
-//   phase 1..3: U stage s and V stage s side by side, each followed by its boundary pass
+//   phase 1..3: U stage s and V stage s side by side, each followed by its boundary pass; in
+//               phases 1 and 2 also T, C stages 2 and 3 of the previous iteration
 //   phase 4   : P (the three stages fuse pointwise) and T, C stage 1
-//   phase 5..6: T, C stages 2, 3
-//   control   : every CTA reads the case's residual maxima and takes the same decision
+//   control   : every CTA reads the case's residual maxima and takes the same decision; on
+//               exit the pending T, C stages 2 and 3 run on their own first
 // The boundary passes bcUV(u_stage, vm_tau) and bcUV(um_tau, v_stage) also rewrite the boundary
 // of vm_tau / um_tau (boundary.f90:1-49).  Those arrays come from earlier boundary passes, so the
 // rewrite changes nothing -- except right after the state was uploaded.  An iteration with
@@ -41,7 +42,33 @@ struct EngineArgs {
   const int* cases;  // case id per cluster
   int* iters;        // [case * n_steps + step]
   double* err;
+  int stage_elems;   // staged engine: doubles per shared-memory slot (>= (strip rows + 4) * pitch)
 };
+
+// Staged engine: each phase first copies the rows [r0-2, r1+2) of the arrays it reads with a
+// stencil into shared-memory slots (cp.async, 16-byte chunks through L2), then computes from
+// them.  One L2 round trip per phase replaces the dependent L2 loads of every node.
+constexpr int STAGE_SLOTS = 7;
+
+// Issues the copy of rows [ra, rb) of a case array into `slot` and returns a pointer that indexes
+// like the global array for those rows.  Rows start on 32-byte boundaries (the pitch is a
+// multiple of 4 doubles), so every 16-byte chunk is aligned on both sides.
+__device__ __forceinline__ const double* stage_rows(const double* g, double* slot, int ra, int rb, int P) {
+  const long long o = (long long)(ra - 1) * P;
+  const int n16 = ((rb - ra) * P) >> 1;
+  const char* src = reinterpret_cast<const char*>(g + o);
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(slot);
+  for (int q = threadIdx.x; q < n16; q += blockDim.x)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16u * (unsigned)q),
+                 "l"(src + 16 * (long long)q)
+                 : "memory");
+  return slot - o;
+}
+// Completes this thread's copies, then makes every thread's copies visible to the CTA.
+__device__ __forceinline__ void stage_wait() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+}
 
 struct LocalCtl {
   int ru[3], rv[3], rt[3], rc[3], rp[2];
@@ -68,6 +95,28 @@ __device__ __forceinline__ void for_nodes(const Strip& s, int ia, int ib, int ja
   if (j1 < j0 || w <= 0) return;
   const int n = w * (j1 - j0 + 1);
   for (int q = threadIdx.x; q < n; q += blockDim.x) f(ia + q % w, j0 + q / w);
+}
+
+// Same node set, two nodes per thread and trip: g(i, j) (loads and arithmetic only) runs for both
+// nodes before h(i, j, g) stores either result, so the loads of the two nodes are in flight
+// together.  The second node repeats the first when the count is odd (g has no side effects).
+template <class G, class H>
+__device__ __forceinline__ void for_nodes_pair(const Strip& s, int ia, int ib, int ja, int jb, G g, H h) {
+  const int j0 = s.lo(ja), j1 = s.hi(jb);
+  const int w = ib - ia + 1;
+  if (j1 < j0 || w <= 0) return;
+  const int n = w * (j1 - j0 + 1);
+  const int bd = blockDim.x;
+  for (int q = threadIdx.x; q < n; q += 2 * bd) {
+    const int q2 = q + bd;
+    const bool two = q2 < n;
+    const int i1 = ia + q % w, jj1 = j0 + q / w;
+    const int i2 = two ? ia + q2 % w : i1, jj2 = two ? j0 + q2 / w : jj1;
+    const double a1 = g(i1, jj1);
+    const double a2 = g(i2, jj2);
+    h(i1, jj1, a1);
+    if (two) h(i2, jj2, a2);
+  }
 }
 
 template <class F>
@@ -182,13 +231,19 @@ __device__ inline void block_max3(double a, double b, double c, unsigned long lo
 // PT provides the per-node residuals: ru(d, uin, vt, pn, i, j), rv(d, ut, vin, pn, T, i, j),
 // rs<IS_C>(d, un, vn, z, i, j), p_update(d, p0, un, vn, i, j, &r), and ld(ptr, q), the load used
 // for arrays that other CTAs of the cluster write.
-template <class PT, int NT, int MINB = 1>
+template <class PT, int NT, int MINB = 1, bool STG = false>
 __global__ void __launch_bounds__(NT, MINB) k_engine(EngineArgs a) {
+  extern __shared__ __align__(16) double stg_smem[];
   cg::cluster_group cl = cg::this_cluster();
   const int K = (int)cl.num_blocks();
   const int rank = (int)cl.block_rank();
   const int c = a.cases[blockIdx.x / K];
-  const CaseDev& d = a.cs[c];
+  // the case's constants and buffer pointers in shared memory: reads of them neither go to L1/L2
+  // nor have to be repeated after every global store (a global store cannot alias them)
+  __shared__ CaseDev d_sh;
+  if (threadIdx.x == 0) d_sh = a.cs[c];
+  __syncthreads();
+  const CaseDev& d = d_sh;
   CaseCtl* gk = a.ctl + c;
 
   LocalCtl k;
@@ -204,24 +259,94 @@ __global__ void __launch_bounds__(NT, MINB) k_engine(EngineArgs a) {
   const int nx = d.nx, ny = d.ny;
   const bool scal = k.scalars && d.solve_scalars;
   unsigned long long* slots = gk->slot[0];
+  const int ra = s.r0 - 2 > 1 ? s.r0 - 2 : 1;
+  const int rb = s.r1 + 2 < R + 1 ? s.r1 + 2 : R + 1;
+  auto stage = [&](int slot, const double* g) -> const double* {
+    if constexpr (STG) return stage_rows(g, stg_smem + (long long)slot * a.stage_elems, ra, rb, d.pitch);
+    else return g;
+  };
+  auto stage_done = [&]() {
+    if constexpr (STG) stage_wait();
+  };
+
+  // T and C of iteration k read only the new velocities of iteration k, and U, V read only the
+  // physical-step T, so T/C stages 2 and 3 of iteration k run during the U/V stages 1 and 2 of
+  // iteration k+1 (four cluster barriers per pseudo-iteration instead of six).  `tb` holds the
+  // buffers of the pending T/C work; on exit (or at itc_max) the pending stages run first.
+  struct TcBufs { const double* un; const double* vn; const double* tau[2]; const double* phys[2]; double* out[2]; };
+  TcBufs tb{};
+  bool pend = false;
+  // zs[v] / us / vs: staged copies of the stage input and of the velocities (null: global arrays)
+  auto tc_stage = [&](const TcBufs& b, int st, const double* const* zs, const double* us, const double* vs) {
+    const double* un = us ? us : b.un;
+    const double* vn = vs ? vs : b.vn;
+    for (int v = 0; v < 2; ++v) {
+      const bool isc = v == 1;
+      const double* zin = zs && zs[v] ? zs[v] : (st == 1 ? b.tau[v] : d.S2[2 * v + st - 2]);
+      double* zout = st == 3 ? b.out[v] : d.S2[2 * v + st - 1];
+      const double* ztau = b.tau[v];
+      const double* z = b.phys[v];
+      for_nodes_pair(s, 2, nx - 1, 2, ny - 1, [&](int i, int j) {
+        return isc ? PT::template rs<true>(d, un, vn, zin, i, j) : PT::template rs<false>(d, un, vn, zin, i, j);
+      }, [&](int i, int j, double Rz) {
+        const long long q = lin(i, j, d.pitch);
+        const double r = ((PT::ld(z, q) - PT::ld(ztau, q)) + Rz * d.dt) * d.dtau;
+        if (st == 1) zout[q] = PT::ld(ztau, q) + r;
+        else if (st == 2) zout[q] = 0.75 * PT::ld(ztau, q) + 0.25 * (PT::ld(zin, q) + r);
+        else zout[q] = 1.0 / 3.0 * PT::ld(ztau, q) + 2.0 / 3.0 * (PT::ld(zin, q) + r);
+      });
+    }
+  };
+  // boundary passes of T/C stage st (callers put a __syncthreads before)
+  auto tc_bc = [&](const TcBufs& b, int st) {
+    strip_bc_cell(d, s, st == 3 ? b.out[0] : d.S2[st - 1], false, d.T_in);
+    __syncthreads();
+    strip_bc_cell(d, s, st == 3 ? b.out[1] : d.S2[2 + st - 1], false, d.C_in);
+  };
+  // the pending stages 2 and 3 on their own (end of a physical step)
+  auto tc_tail = [&]() {
+    for (int st = 2; st <= 3; ++st) {
+      tc_stage(tb, st, nullptr, nullptr, nullptr);
+      __syncthreads();
+      tc_bc(tb, st);
+      cl.sync();
+    }
+    pend = false;
+  };
 
   for (int it = 0;; ++it) {
     unsigned long long* slot = slots + 3 * (it & 1);
     double mu = 0.0, mv = 0.0, mp = 0.0;
     const double* pn_read = d.P[k.rp_read];
-    // ---- U and V, three stages ----
+    // ---- U and V, three stages (with T/C stages 2, 3 of the previous iteration) ----
     const bool seq = k.tau_dirty;
+    if (seq && pend) tc_tail();
     for (int pass = 0; pass < (seq ? 2 : 1); ++pass) {
       const bool doU = !seq || pass == 0, doV = !seq || pass == 1;
       for (int st = 1; st <= 3; ++st) {
+        const bool tc = pend && st <= 2;
+        // arrays read with a stencil in this phase, staged (or the global arrays themselves)
+        const double* g_ut = d.U[k.ru[R_TAU]];
+        const double* g_vt = d.V[k.rv[R_TAU]];
+        const double* s_ut = stage(0, g_ut);
+        const double* s_vt = stage(1, g_vt);
+        const double* s_pn = stage(2, pn_read);
+        const double* s_uin = st == 1 ? s_ut : stage(3, d.S[st - 2]);
+        const double* s_vin = st == 1 ? s_vt : stage(4, d.S[2 + st - 2]);
+        const double* s_z[2] = {nullptr, nullptr};
+        if (tc) {
+          s_z[0] = stage(5, d.S2[st - 1]);
+          s_z[1] = stage(6, d.S2[2 + st - 1]);
+        }
+        stage_done();
         if (doU) {
-          const double* uin = st == 1 ? d.U[k.ru[R_TAU]] : d.S[st - 2];
+          const double* uin = s_uin;
           double* uout = st == 3 ? d.U[k.ru[R_NTAU]] : d.S[st - 1];
-          const double* utau = d.U[k.ru[R_TAU]];
+          const double* utau = g_ut;
           const double* um = d.U[k.ru[R_PHYS]];
-          const double* vt = d.V[k.rv[R_TAU]];
-          for_nodes(s, 3, nx - 1, 2, ny - 1, [&](int i, int j) {
-            const double RU = PT::ru(d, uin, vt, pn_read, i, j);
+          const double* vt = s_vt;
+          for_nodes_pair(s, 3, nx - 1, 2, ny - 1, [&](int i, int j) { return PT::ru(d, uin, vt, s_pn, i, j); },
+                         [&](int i, int j, double RU) {
             const long long q = lin(i, j, d.pitch);
             const double r = ((PT::ld(um, q) - PT::ld(utau, q)) + RU * d.dt) * d.dtau;
             if (st == 1) uout[q] = PT::ld(utau, q) + r;
@@ -234,14 +359,14 @@ __global__ void __launch_bounds__(NT, MINB) k_engine(EngineArgs a) {
           });
         }
         if (doV) {
-          const double* vin = st == 1 ? d.V[k.rv[R_TAU]] : d.S[2 + st - 2];
+          const double* vin = s_vin;
           double* vout = st == 3 ? d.V[k.rv[R_NTAU]] : d.S[2 + st - 1];
-          const double* vtau = d.V[k.rv[R_TAU]];
+          const double* vtau = g_vt;
           const double* vm = d.V[k.rv[R_PHYS]];
-          const double* ut = d.U[k.ru[R_TAU]];
+          const double* ut = s_ut;
           const double* T = d.T[k.rt[R_PHYS]];
-          for_nodes(s, 2, nx - 1, 3, ny - 1, [&](int i, int j) {
-            const double RV = PT::rv(d, ut, vin, pn_read, T, i, j);
+          for_nodes_pair(s, 2, nx - 1, 3, ny - 1, [&](int i, int j) { return PT::rv(d, ut, vin, s_pn, T, i, j); },
+                         [&](int i, int j, double RV) {
             const long long q = lin(i, j, d.pitch);
             const double r = ((PT::ld(vm, q) - PT::ld(vtau, q)) + RV * d.dt) * d.dtau;
             if (st == 1) vout[q] = (PT::ld(vtau, q) + r);
@@ -253,9 +378,16 @@ __global__ void __launch_bounds__(NT, MINB) k_engine(EngineArgs a) {
             }
           });
         }
+        // the pending T/C work reads the previous iteration's new velocities, which after the
+        // role swap are this iteration's tau arrays
+        if (tc) tc_stage(tb, st + 1, s_z, tb.un == g_ut ? s_ut : nullptr, tb.vn == g_vt ? s_vt : nullptr);
         __syncthreads();
         if (doU) strip_bc_u(d, s, st == 3 ? d.U[k.ru[R_NTAU]] : d.S[st - 1]);
         if (doV) strip_bc_v(d, s, st == 3 ? d.V[k.rv[R_NTAU]] : d.S[2 + st - 1]);
+        if (tc) {
+          __syncthreads();
+          tc_bc(tb, st + 1);
+        }
         if (seq) {
           // bcUV(u_stage, vm_tau) / bcUV(um_tau, v_stage) also rewrite vm_tau / um_tau, which
           // other CTAs may still be reading for this stage: wait for the whole cluster first
@@ -264,6 +396,7 @@ __global__ void __launch_bounds__(NT, MINB) k_engine(EngineArgs a) {
           else strip_bc_u(d, s, d.U[k.ru[R_TAU]]);
         }
         cl.sync();
+        if (tc && st == 2) pend = false;
         // the residual slot of the next iteration is free once every CTA is past the control
         // step of the previous one, i.e. after the first barrier of this iteration
         if (st == 1 && pass == 0 && rank == 0 && threadIdx.x == 0) {
@@ -275,49 +408,40 @@ __global__ void __launch_bounds__(NT, MINB) k_engine(EngineArgs a) {
     // ---- P, and T / C stage 1 ----
     const double* un = d.U[k.ru[R_NTAU]];
     const double* vn = d.V[k.rv[R_NTAU]];
+    const double* s_un = stage(0, un);
+    const double* s_vn = stage(1, vn);
+    const double* s_z4[2] = {nullptr, nullptr};
+    if (scal) {
+      s_z4[0] = stage(2, d.T[k.rt[R_TAU]]);
+      s_z4[1] = stage(3, d.C[k.rc[R_TAU]]);
+    }
+    stage_done();
     {
       const double* p0 = d.P[k.rp[0]];
       double* pn = d.P[k.rp[1]];
       for_nodes(s, 2, nx - 1, 2, ny - 1, [&](int i, int j) {
         double r;
-        pn[lin(i, j, d.pitch)] = PT::p_update(d, p0, un, vn, i, j, &r);
+        pn[lin(i, j, d.pitch)] = PT::p_update(d, p0, s_un, s_vn, i, j, &r);
         const double ar = fabs(r);
         mp = (ar > mp || ar != ar) ? ar : mp;
       });
     }
-    for (int st = 1; st <= (scal ? 3 : 0); ++st) {
-      for (int v = 0; v < 2; ++v) {
-        const bool isc = v == 1;
-        double* const* F = isc ? d.C : d.T;
-        const int* rr = isc ? k.rc : k.rt;
-        const double* zin = st == 1 ? F[rr[R_TAU]] : d.S[2 * v + st - 2];
-        double* zout = st == 3 ? F[rr[R_NTAU]] : d.S[2 * v + st - 1];
-        const double* ztau = F[rr[R_TAU]];
-        const double* z = F[rr[R_PHYS]];
-        for_nodes(s, 2, nx - 1, 2, ny - 1, [&](int i, int j) {
-          const double Rz = isc ? PT::template rs<true>(d, un, vn, zin, i, j) : PT::template rs<false>(d, un, vn, zin, i, j);
-          const long long q = lin(i, j, d.pitch);
-          const double r = ((PT::ld(z, q) - PT::ld(ztau, q)) + Rz * d.dt) * d.dtau;
-          if (st == 1) zout[q] = PT::ld(ztau, q) + r;
-          else if (st == 2) zout[q] = 0.75 * PT::ld(ztau, q) + 0.25 * (PT::ld(zin, q) + r);
-          else zout[q] = 1.0 / 3.0 * PT::ld(ztau, q) + 2.0 / 3.0 * (PT::ld(zin, q) + r);
-        });
-      }
-      __syncthreads();
-      if (st == 1) strip_bc_cell(d, s, d.P[k.rp[1]], true, 0.0);
-      __syncthreads();
-      strip_bc_cell(d, s, st == 3 ? d.T[k.rt[R_NTAU]] : d.S[st - 1], false, d.T_in);
-      __syncthreads();
-      strip_bc_cell(d, s, st == 3 ? d.C[k.rc[R_NTAU]] : d.S[2 + st - 1], false, d.C_in);
-      if (st == 1) block_max3(mu, mv, mp, slot);
-      cl.sync();
+    if (scal) {
+      tb.un = un;
+      tb.vn = vn;
+      tb.tau[0] = d.T[k.rt[R_TAU]]; tb.phys[0] = d.T[k.rt[R_PHYS]]; tb.out[0] = d.T[k.rt[R_NTAU]];
+      tb.tau[1] = d.C[k.rc[R_TAU]]; tb.phys[1] = d.C[k.rc[R_PHYS]]; tb.out[1] = d.C[k.rc[R_NTAU]];
+      tc_stage(tb, 1, s_z4, s_un, s_vn);
     }
-    if (!scal) {
+    __syncthreads();
+    strip_bc_cell(d, s, d.P[k.rp[1]], true, 0.0);
+    if (scal) {
       __syncthreads();
-      strip_bc_cell(d, s, d.P[k.rp[1]], true, 0.0);
-      block_max3(mu, mv, mp, slot);
-      cl.sync();
+      tc_bc(tb, 1);
+      pend = true;
     }
+    block_max3(mu, mv, mp, slot);
+    cl.sync();
     // ---- control (main.f90:139-157), identical in every CTA ----
     const double ru = __longlong_as_double((long long)__ldcg(slot + 0));
     const double rv = __longlong_as_double((long long)__ldcg(slot + 1));
@@ -333,6 +457,7 @@ __global__ void __launch_bounds__(NT, MINB) k_engine(EngineArgs a) {
       k.active = 0;
       step_done = true;
     } else if (k.itc != 1 && e < d.eps) {
+      if (pend) tc_tail();
       k.rp_read = k.rp[1];
       k.ntau_alias = 1;
       swap_l(k.ru[R_PHYS], k.ru[R_NTAU]);
@@ -351,6 +476,7 @@ __global__ void __launch_bounds__(NT, MINB) k_engine(EngineArgs a) {
       if (k.itc >= d.itc_max) { copy = true; step_done = true; }
     }
     if (copy) {  // loop condition failed after the copies: phys = latest iterate (main.f90:154-157)
+      if (pend) tc_tail();
       const int nf = d.solve_scalars ? 4 : 2;
       for (int f = 0; f < nf; ++f) {
         const double* src = f == 0 ? d.U[k.ru[R_TAU]] : f == 1 ? d.V[k.rv[R_TAU]] : f == 2 ? d.T[k.rt[R_TAU]] : d.C[k.rc[R_TAU]];

@@ -36,6 +36,9 @@ __device__ __forceinline__ Met my(const CaseDev& d, int j) {
 // cluster barrier's release/acquire pair orders the writes before the reads in both cases.
 struct LdL2 { static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldcg(a + q); } };
 struct LdL1 { static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldca(a + q); } };
+// Generic loads: the staged engine reads its stencil arrays from shared memory and the rest from
+// global memory written by this CTA or before the cluster barrier.
+struct LdGen { static __device__ __forceinline__ double ld(const double* a, long long q) { return a[q]; } };
 
 // QUICK face value seen from the face's upstream side (equations.f90:27-70 rearranged):
 // flux > 0 takes 0.75 of the upwind node, 0.375 of the downwind node, -0.125 of the far upwind.
@@ -160,16 +163,23 @@ struct PtFastT {
 
 using PtFast = PtFastT<LdL2>;
 using PtFastL1 = PtFastT<LdL1>;
+using PtFastGen = PtFastT<LdGen>;
 
 namespace {
-template <class PT, int NT, int MINB>
+template <class PT, int NT, int MINB, bool STG = false>
 cudaError_t launch_fast_t(const EngineArgs& a, int cluster, int nclusters, cudaStream_t s) {
-  auto kern = k_engine<PT, NT, MINB>;
+  auto kern = k_engine<PT, NT, MINB, STG>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;
+  const size_t smem = STG ? (size_t)STAGE_SLOTS * a.stage_elems * sizeof(double) : 0;
+  if (STG) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cluster * nclusters);
   cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -183,9 +193,14 @@ cudaError_t launch_fast_t(const EngineArgs& a, int cluster, int nclusters, cudaS
 }  // namespace
 
 // threads: 256 or 512 per CTA; ctas_per_sm: 2 caps a 256-thread CTA at 128 registers so two
-// CTAs of different clusters share an SM; l1: load cluster-written arrays through L1
+// CTAs of different clusters share an SM; l1: load cluster-written arrays through L1; staged:
+// stage the stencil arrays in shared memory (a.stage_elems doubles per slot, one CTA per SM)
 cudaError_t launch_engine_fast(const EngineArgs& a, int cluster, int nclusters, cudaStream_t s, int l1, int threads,
-                               int ctas_per_sm) {
+                               int ctas_per_sm, int staged) {
+  if (staged) {
+    if (threads == 512) return launch_fast_t<PtFastGen, 512, 1, true>(a, cluster, nclusters, s);
+    return launch_fast_t<PtFastGen, 256, 1, true>(a, cluster, nclusters, s);
+  }
   if (threads == 512)
     return l1 ? launch_fast_t<PtFastL1, 512, 1>(a, cluster, nclusters, s) : launch_fast_t<PtFast, 512, 1>(a, cluster, nclusters, s);
   if (ctas_per_sm == 2)

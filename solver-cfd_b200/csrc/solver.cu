@@ -42,6 +42,7 @@ int fail(int code, const std::string& msg) {
 namespace {
 
 constexpr int kMinN = 6;
+constexpr long long kMaxStageBytes = 220 * 1024;  // dynamic shared memory for the staged engine
 constexpr int kMaxN = 1 << 15;
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -102,6 +103,8 @@ struct Batch {
   int l1_loads = 1;      // FAST engine: load cluster-written arrays through L1
   int threads = 512;     // FAST engine: threads per CTA (256 or 512)
   int ctas_per_sm = 1;   // FAST engine with 256 threads: 1 or 2 resident CTAs per SM
+  int staged = 1;        // FAST engine: stage stencil arrays in shared memory where they fit
+  int last_staged = 0;   // the last engine launch used the staged kernel
   int* d_cases = nullptr;
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> ev;
@@ -331,7 +334,7 @@ int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch**
     const int nx = params[c].imax, ny = params[c].jmax;
     const size_t ne = align_up(nx + 1, 4) * (size_t)(ny + 1);
     size_t sz = align_up(sizeof(double) * (2 * nx + 2 * ny + 6), 256) + 2 * align_up(8 * ne, 256) +
-                align_up(ne, 256) + 18 * align_up(8 * ne, 256);
+                align_up(ne, 256) + 22 * align_up(8 * ne, 256);
     off[c] = total;
     sizes[c] = sz;
     total += align_up(sz, 256);
@@ -436,6 +439,7 @@ int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch**
         q += align_up(8 * ne, 256);
       }
     for (int r = 0; r < 4; ++r) { d.S[r] = (double*)q; q += align_up(8 * ne, 256); }
+    for (int r = 0; r < 4; ++r) { d.S2[r] = (double*)q; q += align_up(8 * ne, 256); }
     reset_roles(b->hk[c]);
   }
   if (fast) {
@@ -718,9 +722,19 @@ int run_engine(Batch& b) {
     const int cnt = (int)groups[K].size();
     cudaStream_t s = g == 0 ? b.stream : b.side[g];
     if (g) CU(cudaStreamWaitEvent(s, fork, 0));
-    EngineArgs a{b.dc, b.dk, b.d_cases + off, b.d_iters, b.d_err};
-    cudaError_t e = b.use_fast ? launch_engine_fast(a, K, cnt, s, b.l1_loads, b.threads, b.ctas_per_sm)
+    // staging slot: the largest strip of the size class plus two halo rows on each side
+    long long slot = 0;
+    for (int q = 0; q < cnt; ++q) {
+      const CaseDev& d = b.hc[order[off + q]];
+      const long long rows = (d.ny + 1 + K - 1) / K + 4;
+      slot = std::max(slot, (rows * d.pitch + 1) / 2 * 2);
+    }
+    const bool stg = b.use_fast && b.staged && b.ctas_per_sm == 1 &&
+                     (long long)STAGE_SLOTS * slot * 8 <= kMaxStageBytes;
+    EngineArgs a{b.dc, b.dk, b.d_cases + off, b.d_iters, b.d_err, stg ? (int)slot : 0};
+    cudaError_t e = b.use_fast ? launch_engine_fast(a, K, cnt, s, b.l1_loads, b.threads, b.ctas_per_sm, stg ? 1 : 0)
                                : launch_engine_exact(a, K, cnt, s);
+    b.last_staged = stg ? 1 : 0;
     if (e != cudaSuccess) {
       cudaEventDestroy(fork);
       return fail(ACS_E_CUDA, std::string("engine launch (cluster ") + std::to_string(K) + "): " + cudaGetErrorString(e));
@@ -975,6 +989,9 @@ int acs_batch_set_option(acs_batch* h, int option, long long value) {
     case ACS_OPT_CTAS_PER_SM:
       if (value != 1 && value != 2) return acs::fail(ACS_E_ARG, "CTAs per SM must be 1 or 2");
       b.ctas_per_sm = (int)value;
+      return ACS_OK;
+    case ACS_OPT_STAGED:
+      b.staged = value ? 1 : 0;
       return ACS_OK;
   }
   return acs::fail(ACS_E_ARG, "unknown option");
