@@ -47,6 +47,12 @@ int unet_f32_to_bf16(const float* a, long long n, void* b, void* stream);
 /* *loss += sum w (out - tgt)^2 * inv_norm, dout = 2 w (out - tgt) inv_norm (loss zeroed by the caller) */
 int unet_mse(const float* out, const float* tgt, const float* w, long long n, float inv_norm, float* dout,
              float* loss, void* stream);
+/* as unet_mse on an NHWC [B][H][W][C] tensor, plus lam x the squared differences of the error
+ * between x- and y-neighbours that both have weight (loss and gradient) */
+int unet_mse_grad(const float* out, const float* tgt, const float* w, int B, int H, int W, int C, float lam,
+                  float inv_norm, float* dout, float* loss, void* stream);
+/* Y = 3 x 3 box mean of X per channel (NHWC FP32; edges average the existing neighbours; Y != X) */
+int unet_smooth3(const float* X, int B, int H, int W, int C, float* Y, void* stream);
 /* y = (x - shift[c]) * mul[c] over M pixels x C channels (FP32 in) to Y_bf16 and/or Y_f32 (either may be
  * NULL, not both; Y_f32 may alias X) */
 int unet_normalize(const float* X, long long M, int C, const float* shift, const float* mul, void* Y_bf16,

@@ -62,6 +62,9 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=100)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--grad-weight", type=float, default=0.0,
+                    help="weight of the squared x/y differences of the error in the loss")
+    ap.add_argument("--smooth", type=int, default=0, help="3x3 box passes over the network output")
     ap.add_argument("--eval-cases", type=int, default=4)
     ap.add_argument("--eval-steps", type=int, default=10)
     ap.add_argument("--seed", type=int, default=100)
@@ -86,6 +89,8 @@ def main(argv=None):
     if a.load:
         net, norm, H2, W2, meta = ws.load(a.load)
         assert (H2, W2) == (H, W)
+        if a.smooth:
+            norm.smooth = a.smooth
         report["trained"] = meta
     else:
         cases = make_cases(pkg, a.n, a.train_cases, a.seed, arith)
@@ -98,12 +103,13 @@ def main(argv=None):
         norm = ws.Normalizer.from_samples(X[:take].cpu().numpy().reshape(-1, H, W, 11),
                                           T[:take].cpu().numpy().reshape(-1, H, W, 8),
                                           Wt[:take].cpu().numpy().reshape(-1, H, W, 8))
+        norm.smooth = a.smooth
         net = unet.UNet(11, 5, 32, 4, seed=a.seed)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
         losses = ws.train(net, X, T, Wt, H, W, norm, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed,
-                          log=log)
+                          log=log, grad_weight=a.grad_weight)
         e1.record()
         torch.cuda.synchronize()
         train_s = e0.elapsed_time(e1) / 1e3

@@ -41,6 +41,8 @@ _SIG = {
     "unet_bias_grad": [V, LL, I, V, V],
     "unet_f32_to_bf16": [V, LL, V, V],
     "unet_mse": [V, V, V, LL, F, V, V, V],
+    "unet_mse_grad": [V, V, V, I, I, I, I, F, F, V, V, V],
+    "unet_smooth3": [V, I, I, I, I, V, V],
     "unet_normalize": [V, LL, I, V, V, V, V, V],
     "unet_adam": [V, V, V, V, LL, F, F, F, F, I, V, V],
 }
@@ -349,15 +351,20 @@ class UNet:
             dxin = G[f"P{l - 1}"] if l > 0 else None
             self._conv_bwd(ws, self.by_name[f"enc{l}a"], xin, A[f"a{l}"], G[f"a{l}"], dxin, l)
 
-    def loss(self, target, weight, inv_norm):
-        """Masked MSE of the last forward output against target (FP32 [B*H*W*8]); writes
-        dLoss/dY into the workspace and returns the loss as a device scalar."""
+    def loss(self, target, weight, inv_norm, lam=0.0):
+        """Masked MSE of the last forward output against target (FP32 [B*H*W*8]), plus lam x the
+        squared x/y differences of the error when lam > 0; writes dLoss/dY into the workspace and
+        returns the loss as a device scalar."""
         ws = self._last
         K = kernels()
         ws["loss"].zero_()
         n = ws["y"].numel()
-        _ok(K.unet_mse(_p(ws["y"]), _p(target), _p(weight), n, float(inv_norm), _p(ws["dy"]), _p(ws["loss"]),
-                       self._stream()), "mse")
+        if lam > 0.0:
+            _ok(K.unet_mse_grad(_p(ws["y"]), _p(target), _p(weight), ws["B"], ws["H"], ws["W"], OUT_PAD, float(lam),
+                                float(inv_norm), _p(ws["dy"]), _p(ws["loss"]), self._stream()), "mse_grad")
+        else:
+            _ok(K.unet_mse(_p(ws["y"]), _p(target), _p(weight), n, float(inv_norm), _p(ws["dy"]), _p(ws["loss"]),
+                           self._stream()), "mse")
         return ws["loss"]
 
     def adam(self, lr, b1=0.9, b2=0.999, eps=1e-8):
@@ -367,10 +374,10 @@ class UNet:
                         self.t, _p(self.wt_bf16), self._stream()), "adam")
         self._transpose_weights()
 
-    def train_step(self, B, H, W, target, weight, inv_norm, lr, X_bf16=None):
-        """forward + masked MSE + backward + Adam; returns the loss (device scalar)."""
+    def train_step(self, B, H, W, target, weight, inv_norm, lr, X_bf16=None, lam=0.0):
+        """forward + masked MSE (+ difference term) + backward + Adam; returns the loss."""
         self.forward(B, H, W, X_bf16)
-        loss = self.loss(target, weight, inv_norm)
+        loss = self.loss(target, weight, inv_norm, lam)
         self.backward()
         self.adam(lr)
         return loss

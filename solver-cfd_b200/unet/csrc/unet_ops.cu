@@ -39,6 +39,24 @@ __global__ void k_im2col(const bf16* __restrict__ X, int B, int H, int W, int C,
   }
 }
 
+// C a multiple of 8 (then Kp = 9C): one thread per 16-byte vector of 8 channels of one tap of one
+// pixel, consecutive threads on consecutive vectors (coalesced loads and stores)
+__global__ void k_im2col_v8(const uint4* __restrict__ X, int B, int H, int W, int C, uint4* __restrict__ col) {
+  const int C8 = C >> 3;
+  const long long n = (long long)B * H * W * 9 * C8;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(q % (9 * C8));
+    const long long m = q / (9 * C8);
+    const int tap = r / C8, c8 = r - tap * C8;
+    const int ky = tap / 3, kx = tap - ky * 3;
+    const int x = (int)(m % W), y = (int)((m / W) % H), b = (int)(m / ((long long)W * H));
+    const int yy = y + ky - 1, xx = x + kx - 1;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (yy >= 0 && yy < H && xx >= 0 && xx < W) v = X[(((long long)b * H + yy) * W + xx) * C8 + c8];
+    col[q] = v;
+  }
+}
+
 __global__ void k_col2im(const float* __restrict__ dcol, int B, int H, int W, int C, int Kp, float* __restrict__ dX) {
   const long long n = (long long)B * H * W * C;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
@@ -179,6 +197,56 @@ __global__ void k_mse(const float* __restrict__ out, const float* __restrict__ t
   if ((threadIdx.x & 31) == 0) atomicAdd(loss, s * inv_norm);
 }
 
+// masked mean-square error plus lam x the squared first differences of the error along x and y
+// (a difference counts where both nodes have weight): the residual of a predicted start is a
+// differential operator of its error, so the loss also asks for accurate differences.
+// One thread per (pixel, channel) of an NHWC [B][H][W][C] tensor.
+__global__ void k_mse_grad(const float* __restrict__ out, const float* __restrict__ tgt, const float* __restrict__ w,
+                           int B, int H, int W, int C, float lam, float inv_norm, float* __restrict__ dout,
+                           float* __restrict__ loss) {
+  const long long n = (long long)B * H * W * C;
+  float s = 0.f;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(q % C);
+    const long long p = q / C;
+    const int x = (int)(p % W), y = (int)((p / W) % H);
+    const float wq = w[q];
+    const float e = wq > 0.f ? out[q] - tgt[q] : 0.f;
+    float g = 2.f * wq * e;
+    s += wq * e * e;
+    if (wq > 0.f) {
+      const long long qe = q + C, qw = q - C, qn = q + (long long)W * C, qs = q - (long long)W * C;
+      if (x + 1 < W && w[qe] > 0.f) { const float d = (out[qe] - tgt[qe]) - e; s += lam * d * d; g -= 2.f * lam * d; }
+      if (x > 0 && w[qw] > 0.f) { const float d = e - (out[qw] - tgt[qw]); g += 2.f * lam * d; }
+      if (y + 1 < H && w[qn] > 0.f) { const float d = (out[qn] - tgt[qn]) - e; s += lam * d * d; g -= 2.f * lam * d; }
+      if (y > 0 && w[qs] > 0.f) { const float d = e - (out[qs] - tgt[qs]); g += 2.f * lam * d; }
+    }
+    dout[q] = g * inv_norm;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, s * inv_norm);
+}
+
+// 3 x 3 box mean of every channel over the canvas (edges average the neighbours that exist)
+__global__ void k_smooth3(const float* __restrict__ X, int B, int H, int W, int C, float* __restrict__ Y) {
+  const long long n = (long long)B * H * W * C;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(q % C);
+    const long long p = q / C;
+    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+    float s = 0.f;
+    int k = 0;
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int yy = y + dy, xx = x + dx;
+        if (yy < 0 || yy >= H || xx < 0 || xx >= W) continue;
+        s += X[(((long long)b * H + yy) * W + xx) * C + c];
+        ++k;
+      }
+    Y[q] = s / (float)k;
+  }
+}
+
 // Adam on FP32 master parameters, refreshing the BF16 copy used by the GEMMs
 __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
                        long long n, float lr, float b1, float b2, float eps, float bc1, float bc2, bf16* __restrict__ pb) {
@@ -219,6 +287,10 @@ extern "C" {
 
 int unet_im2col(const void* X, int B, int H, int W, int C, int Kp, void* col, void* stream) {
   if (!X || !col || Kp < 9 * C || (Kp & 7)) return 1;
+  if ((C & 7) == 0 && Kp == 9 * C && !(reinterpret_cast<uintptr_t>(X) & 15) && !(reinterpret_cast<uintptr_t>(col) & 15)) {
+    k_im2col_v8<<<blocks((long long)B * H * W * 9 * (C >> 3)), T, 0, S_>>>((const uint4*)X, B, H, W, C, (uint4*)col);
+    return ret(S_);
+  }
   k_im2col<<<blocks((long long)B * H * W * Kp), T, 0, S_>>>((const bf16*)X, B, H, W, C, Kp, (bf16*)col);
   return ret(S_);
 }
@@ -283,6 +355,18 @@ int unet_mse(const float* out, const float* tgt, const float* w, long long n, fl
              void* stream) {
   if (!out || !tgt || !w || !dout || !loss) return 1;
   k_mse<<<blocks(n) < 4096 ? blocks(n) : 4096, T, 0, S_>>>(out, tgt, w, n, inv_norm, dout, loss);
+  return ret(S_);
+}
+int unet_mse_grad(const float* out, const float* tgt, const float* w, int B, int H, int W, int C, float lam,
+                  float inv_norm, float* dout, float* loss, void* stream) {
+  if (!out || !tgt || !w || !dout || !loss || B <= 0 || H <= 0 || W <= 0 || C <= 0) return 1;
+  const long long n = (long long)B * H * W * C;
+  k_mse_grad<<<blocks(n) < 4096 ? blocks(n) : 4096, T, 0, S_>>>(out, tgt, w, B, H, W, C, lam, inv_norm, dout, loss);
+  return ret(S_);
+}
+int unet_smooth3(const float* X, int B, int H, int W, int C, float* Y, void* stream) {
+  if (!X || !Y || X == Y || B <= 0 || H <= 0 || W <= 0 || C <= 0) return 1;
+  k_smooth3<<<blocks((long long)B * H * W * C), T, 0, S_>>>(X, B, H, W, C, Y);
   return ret(S_);
 }
 int unet_normalize(const float* X, long long M, int C, const float* shift, const float* mul, void* Y_bf16,

@@ -48,8 +48,9 @@ def valid_nodes(nx: int, ny: int) -> int:
 class Normalizer:
     """Per-channel input shift/scale and output scale (device float vectors)."""
 
-    def __init__(self, in_shift, in_mul, out_scale, device="cuda", inc_weight=None):
+    def __init__(self, in_shift, in_mul, out_scale, device="cuda", inc_weight=None, smooth=0):
         import torch
+        self.smooth = int(smooth)   # 3 x 3 box passes over the network output before it is used
         self.in_shift = torch.tensor(np.asarray(in_shift, np.float32), device=device)
         self.in_mul = torch.tensor(np.asarray(in_mul, np.float32), device=device)
         osc = np.ones(WS_OUT, np.float32)
@@ -87,7 +88,7 @@ class Normalizer:
     def to_dict(self):
         return {"in_shift": self.in_shift.cpu().numpy(), "in_mul": self.in_mul.cpu().numpy(),
                 "out_scale": self.out_scale.cpu().numpy()[:N_FIELDS],
-                "inc_weight": self.out_scale.cpu().numpy()[WS_OUT:]}
+                "inc_weight": self.out_scale.cpu().numpy()[WS_OUT:], "smooth": self.smooth}
 
 
 class WarmStart:
@@ -127,7 +128,25 @@ class WarmStart:
                                              xin.data_ptr(), None, self.torch.cuda.current_stream().cuda_stream)
         if code:
             raise RuntimeError(f"unet_normalize failed with code {code}")
-        return net.forward(self.n, self.H, self.W)
+        y = net.forward(self.n, self.H, self.W)
+        return self.smoothed(y)
+
+    def smoothed(self, y):
+        """`norm.smooth` passes of the 3 x 3 box mean over the network output."""
+        if self.norm.smooth <= 0:
+            return y
+        if getattr(self, "_sm", None) is None or self._sm[0].numel() != y.numel():
+            self._sm = (self.torch.empty_like(y), self.torch.empty_like(y))
+        K = unet_kernels()
+        st = self.torch.cuda.current_stream().cuda_stream
+        src = y
+        for k in range(self.norm.smooth):
+            dst = self._sm[k % 2]
+            code = K.unet_smooth3(src.data_ptr(), self.n, self.H, self.W, WS_OUT, dst.data_ptr(), st)
+            if code:
+                raise RuntimeError(f"unet_smooth3 failed with code {code}")
+            src = dst
+        return src
 
     def step(self, itc, mode: str = "learned"):
         """One physical step of every case.  mode: "plain" (the reference's start), "extrap"
@@ -184,9 +203,10 @@ def generate(batch: Batch, H: int, W: int, n_steps: int, itc, skip: int = 2, mod
 
 
 def train(net: UNet, X, T, Wt, H, W, norm: Normalizer, epochs=10, batch=16, lr=1e-3, seed=0, log=None,
-          lr_final=1e-4):
-    """Minibatch Adam on the snapshots (device tensors from generate()).  Returns the per-epoch
-    mean losses."""
+          lr_final=1e-4, grad_weight=0.0):
+    """Minibatch Adam on the snapshots (device tensors from generate()).  The loss is the masked
+    MSE, plus grad_weight x the squared x/y differences of the error when grad_weight > 0.
+    Returns the per-epoch mean losses."""
     torch = net.torch
     rng = np.random.default_rng(seed)
     K = unet_kernels()
@@ -217,7 +237,7 @@ def train(net: UNet, X, T, Wt, H, W, norm: Normalizer, epochs=10, batch=16, lr=1
             # cosine learning-rate decay from lr to lr_final
             a = 0.5 * (1 + math.cos(math.pi * k / max(1, steps_total)))
             cur = lr_final + (lr - lr_final) * a
-            loss = net.train_step(batch, H, W, tgt, wgt, 1.0 / count, cur)
+            loss = net.train_step(batch, H, W, tgt, wgt, 1.0 / count, cur, lam=grad_weight)
             acc += loss
             nb += 1
             k += 1
@@ -241,7 +261,8 @@ def load(path, device="cuda"):
     net = UNet(int(z["cin"]), int(z["cout"]), int(z["base"]), int(z["levels"]), device=device)
     net.set_params(z["params"])
     norm = Normalizer(z["in_shift"], z["in_mul"], z["out_scale"], device,
-                      z["inc_weight"] if "inc_weight" in z.files else None)
+                      z["inc_weight"] if "inc_weight" in z.files else None,
+                      int(z["smooth"]) if "smooth" in z.files else 0)
     return net, norm, int(z["H"]), int(z["W"]), json.loads(str(z["meta"]))
 
 

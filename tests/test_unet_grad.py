@@ -101,12 +101,13 @@ def test_training_reduces_loss(un):
     assert losses[-1] < 0.3 * losses[0], losses[::10]
 
 
-def test_im2col_col2im_adjoint_and_pool_up(un):
+@pytest.mark.parametrize("Cc", [5, 16])   # scalar path; 16-byte vector path (C multiple of 8)
+def test_im2col_col2im_adjoint_and_pool_up(un, Cc):
     """<im2col(x), c> = <x, col2im(c)>; pooling and upsampling against their definitions."""
     import torch
     K = un.kernels()
     s = torch.cuda.current_stream().cuda_stream
-    B, H, W, Cc = 2, 8, 16, 5
+    B, H, W = 2, 8, 16
     kp = (9 * Cc + 7) // 8 * 8
     g = torch.Generator(device="cuda").manual_seed(3)
     x = torch.randn(B * H * W * Cc, device="cuda", generator=g).to(torch.bfloat16)
@@ -158,3 +159,38 @@ def test_adam_matches_formula(un):
         rp = rp - 1e-2 * (rm / (1 - 0.9 ** t)) / ((rv / (1 - 0.999 ** t)).sqrt() + 1e-8)
     assert (p.double() - rp).abs().max().item() < 1e-5
     assert torch.equal(pb, p.to(torch.bfloat16))
+
+
+def test_difference_loss_and_smoothing(un):
+    """unet_mse_grad: loss and gradient against torch autograd of
+    sum w e^2 + lam sum over valid x/y neighbour pairs of (e' - e)^2 (times inv_norm);
+    unet_smooth3 against a 3x3 mean over the existing neighbours."""
+    import torch
+    K = un.kernels()
+    s = torch.cuda.current_stream().cuda_stream
+    B, H, W, Cc = 2, 9, 12, 8
+    g = torch.Generator(device="cuda").manual_seed(21)
+    out = torch.randn(B, H, W, Cc, device="cuda", generator=g)
+    tgt = torch.randn(B, H, W, Cc, device="cuda", generator=g)
+    w = (torch.rand(B, H, W, Cc, device="cuda", generator=g) < 0.8).float()
+    lam, inv = 3.0, 1.0 / 77.0
+    dout = torch.zeros_like(out)
+    loss = torch.zeros(1, device="cuda")
+    assert K.unet_mse_grad(out.data_ptr(), tgt.data_ptr(), w.data_ptr(), B, H, W, Cc, lam, inv, dout.data_ptr(),
+                           loss.data_ptr(), s) == 0
+    o = out.double().cpu().requires_grad_(True)
+    t, m = tgt.double().cpu(), w.double().cpu()
+    e = (o - t) * (m > 0)
+    ref = (m * e * e).sum()
+    vx = (m[:, :, 1:] > 0) & (m[:, :, :-1] > 0)
+    vy = (m[:, 1:] > 0) & (m[:, :-1] > 0)
+    ref = ref + lam * (((e[:, :, 1:] - e[:, :, :-1]) ** 2) * vx).sum() + lam * (((e[:, 1:] - e[:, :-1]) ** 2) * vy).sum()
+    ref = ref * inv
+    ref.backward()
+    assert abs(float(loss.item()) - float(ref)) <= 1e-4 * abs(float(ref))
+    assert torch.allclose(dout.double().cpu(), o.grad, rtol=1e-4, atol=1e-6)
+    sm = torch.zeros_like(out)
+    assert K.unet_smooth3(out.data_ptr(), B, H, W, Cc, sm.data_ptr(), s) == 0
+    x = out.permute(0, 3, 1, 2)
+    refs = torch.nn.functional.avg_pool2d(x, 3, stride=1, padding=1, count_include_pad=False).permute(0, 2, 3, 1)
+    assert torch.allclose(sm, refs, rtol=1e-5, atol=1e-6)
