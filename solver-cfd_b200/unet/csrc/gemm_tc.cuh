@@ -9,8 +9,9 @@
 // descriptor per 16-wide K step addresses it (leading byte offset = distance between the two
 // K-chunks of a step, stride byte offset = 128 bytes between 8-row groups).  Thread 0 issues
 // tcgen05.mma.cta_group::1.kind::f16 (M = 128, N = BN, K = 16) with the accumulator in tensor
-// memory and commits to an mbarrier; slabs are double buffered so the copy of slab s+1 overlaps
-// the MMAs of slab s.  The epilogue reads the accumulator with tcgen05.ld (32 lanes x 32 bit,
+// memory and commits to an mbarrier per stage.  Three stages: the copies of slabs s+1 and s+2
+// (cp.async groups) are in flight while the MMAs of slab s run, and a stage is refilled once the
+// commit of the MMAs that read it has arrived.  The epilogue reads the accumulator with tcgen05.ld (32 lanes x 32 bit,
 // 16 columns per load): warp w owns TMEM lanes 32w..32w+31, i.e. tile rows 32w..32w+31.
 //
 // Every wait on an mbarrier is bounded; on a timeout the kernel records the failure in *err,
@@ -24,6 +25,7 @@ namespace unet {
 constexpr int TC_BM = 128;
 constexpr int TC_BK = 64;
 constexpr int TC_THREADS = 128;
+constexpr int TC_STAGES = 3;
 constexpr long long TC_WAIT_LIMIT = 1ll << 26;
 
 enum Epilogue {
@@ -90,7 +92,9 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 __device__ __forceinline__ bool cta_wait(uint32_t bar, uint32_t parity, int* flag) {
   if (threadIdx.x == 0) *flag = mbar_wait(bar, parity) ? 1 : 0;
   __syncthreads();
-  return *flag != 0;
+  const bool ok = *flag != 0;
+  __syncthreads();  // every thread has read the flag before thread 0 can write the next one
+  return ok;
 }
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
@@ -114,23 +118,25 @@ __device__ __forceinline__ void load_slab(uint32_t sbase, const __nv_bfloat16* G
 template <int BN, int EPI>
 __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(GemmArgs a) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  // layout: [2 stages][A: 128 x 64][B: BN x 64] bf16, then 2 mbarriers and the TMEM address
+  // layout: [TC_STAGES][A: 128 x 64][B: BN x 64] bf16, then one mbarrier per stage, the TMEM
+  // address and the wait flag
+  constexpr int S = TC_STAGES;
   constexpr int A_BYTES = TC_BM * TC_BK * 2;
   constexpr int B_BYTES = BN * TC_BK * 2;
   constexpr int STAGE = A_BYTES + B_BYTES;
   constexpr int TMEM_COLS = BN < 32 ? 32 : BN;
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + 2 * STAGE);
-  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(smem + 2 * STAGE + 16);
-  int* wait_flag = reinterpret_cast<int*>(smem + 2 * STAGE + 20);
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + S * STAGE);
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(smem + S * STAGE + 8 * S);
+  int* wait_flag = reinterpret_cast<int*>(smem + S * STAGE + 8 * S + 4);
   const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * BN;
   const int kt_total = (a.K + TC_BK - 1) / TC_BK;
   const int kt0 = blockIdx.z * a.k_tiles_per_split;
   const int kt1 = min(kt_total, kt0 + a.k_tiles_per_split);
+  const int nk = kt1 > kt0 ? kt1 - kt0 : 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
-    mbar_init(smem_u32(&bars[0]), 1);
-    mbar_init(smem_u32(&bars[1]), 1);
+    for (int q = 0; q < S; ++q) mbar_init(smem_u32(&bars[q]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -144,19 +150,23 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(GemmArgs a) {
   const uint32_t tmem = *tmem_holder;
   constexpr uint32_t idesc = umma_idesc(TC_BM, BN);
   bool ok = true;
-  uint32_t phase[2] = {0u, 0u};
+  uint32_t phase = 0u;  // bit q: parity of the next completion of stage q's mbarrier
 
-  for (int kt = kt0; kt < kt1; ++kt) {
-    const int s = (kt - kt0) & 1;
-    const uint32_t sa = smem_u32(smem + s * STAGE), sb = sa + A_BYTES;
-    if (kt - kt0 >= 2) {  // the MMAs that last read this stage must be done
-      ok = cta_wait(smem_u32(&bars[s]), phase[s], wait_flag);
-      phase[s] ^= 1u;
-      if (!ok) break;
-    }
-    load_slab(sa, a.A, a.lda, m0, a.M, kt * TC_BK, a.K, TC_BM);
-    load_slab(sb, a.B, a.ldb, n0, a.N, kt * TC_BK, a.K, BN);
-    asm volatile("cp.async.wait_all;" ::: "memory");
+  // slab t of this split goes to stage t % S; cp.async group g holds slab g
+  auto load_tile = [&](int t) {
+    const uint32_t sa = smem_u32(smem + (t % S) * STAGE), sb = sa + A_BYTES;
+    load_slab(sa, a.A, a.lda, m0, a.M, (kt0 + t) * TC_BK, a.K, TC_BM);
+    load_slab(sb, a.B, a.ldb, n0, a.N, (kt0 + t) * TC_BK, a.K, BN);
+  };
+  for (int t = 0; t < S - 1; ++t) {
+    if (t < nk) load_tile(t);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  for (int i = 0; i < nk; ++i) {
+    const int st = i % S;
+    const uint32_t sa = smem_u32(smem + st * STAGE), sb = sa + A_BYTES;
+    // slabs 0..i have landed (at most S-2 newer groups are still in flight)
+    asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -165,7 +175,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(GemmArgs a) {
       for (int ks = 0; ks < TC_BK / 16; ++ks) {
         const uint64_t da = umma_desc(sa + ks * 2 * TC_BM * 16, TC_BM * 16, 128);
         const uint64_t db = umma_desc(sb + ks * 2 * BN * 16, BN * 16, 128);
-        const uint32_t acc = (kt > kt0 || ks > 0) ? 1u : 0u;
+        const uint32_t acc = (i > 0 || ks > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
@@ -173,21 +183,27 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(GemmArgs a) {
             ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                   ::"r"(smem_u32(&bars[s])) : "memory");
+                   ::"r"(smem_u32(&bars[st])) : "memory");
     }
-    __syncthreads();
-  }
-  // wait for the last commit of each stage still outstanding
-  const int nk = kt1 - kt0;
-  if (ok && nk > 0) {
-    for (int s = 0; s < 2; ++s) {
-      const int issued = nk > s ? (nk - s + 1) / 2 : 0;   // commits made on stage s
-      const int waited = nk > 2 + s ? (nk - 2 - s + 1) / 2 : 0;
-      if (issued > waited && ok) {
-        ok = cta_wait(smem_u32(&bars[s]), phase[s], wait_flag);
-        phase[s] ^= 1u;
+    // refill: slab i+S-1 goes to the stage the MMAs of slab i-1 read
+    const int j = i + S - 1;
+    if (j < nk) {
+      if (i >= 1) {
+        const int sp = (i - 1) % S;
+        ok = cta_wait(smem_u32(&bars[sp]), (phase >> sp) & 1u, wait_flag);
+        phase ^= 1u << sp;
+        if (!ok) break;
       }
+      load_tile(j);
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  // the commits of the last min(nk, S) slabs have not been waited for yet (one per stage)
+  for (int t = nk > S ? nk - S : 0; ok && t < nk; ++t) {
+    const int sp = t % S;
+    ok = cta_wait(smem_u32(&bars[sp]), (phase >> sp) & 1u, wait_flag);
+    phase ^= 1u << sp;
   }
   asm volatile("tcgen05.fence::after_thread_sync;");
   if (!ok) {
@@ -204,7 +220,36 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(GemmArgs a) {
             "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < a.M) {
+      const int nb = n0 + c0;
+      const long long o0 = (long long)row * a.ldc + nb;
+      if (EPI == EPI_BIAS_BF16 && row < a.M && nb + 16 <= a.N && (a.ldc & 7) == 0 &&
+          !(reinterpret_cast<uintptr_t>(a.Y) & 15)) {
+        // 16 consecutive columns of one row: two 16-byte stores
+        uint32_t pk[8];
+#pragma unroll
+        for (int j = 0; j < 16; j += 2) {
+          float v0 = __uint_as_float(r[j]) + (a.bias ? a.bias[nb + j] : 0.f);
+          float v1 = __uint_as_float(r[j + 1]) + (a.bias ? a.bias[nb + j + 1] : 0.f);
+          if (a.relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+          const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
+          pk[j >> 1] = *reinterpret_cast<const uint32_t*>(&h);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(a.Y + o0);
+        dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+      } else if ((EPI == EPI_STORE_F32 || EPI == EPI_BIAS_F32) && row < a.M && nb + 16 <= a.N &&
+                 (a.ldc & 3) == 0 && !(reinterpret_cast<uintptr_t>(a.C) & 15)) {
+        float4* dst = reinterpret_cast<float4*>(a.C + o0);
+#pragma unroll
+        for (int j = 0; j < 16; j += 4) {
+          float4 v = make_float4(__uint_as_float(r[j]), __uint_as_float(r[j + 1]), __uint_as_float(r[j + 2]),
+                                 __uint_as_float(r[j + 3]));
+          if (EPI == EPI_BIAS_F32 && a.bias) {
+            v.x += a.bias[nb + j]; v.y += a.bias[nb + j + 1]; v.z += a.bias[nb + j + 2]; v.w += a.bias[nb + j + 3];
+          }
+          dst[j >> 2] = v;
+        }
+      } else if (row < a.M) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int n = n0 + c0 + j;

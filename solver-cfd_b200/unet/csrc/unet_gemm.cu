@@ -9,7 +9,7 @@ namespace {
 
 template <int BN, int EPI>
 cudaError_t go(const GemmArgs& a, int splits, cudaStream_t s) {
-  constexpr int smem = 2 * (TC_BM * TC_BK * 2 + BN * TC_BK * 2) + 64;
+  constexpr int smem = TC_STAGES * (TC_BM * TC_BK * 2 + BN * TC_BK * 2) + 64;
   auto k = k_gemm_tc<BN, EPI>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
