@@ -20,6 +20,13 @@ extern "C" {
 int unet_gemm(const void* A, int lda, const void* B, int ldb, int M, int N, int K, int epilogue,
               float* C, void* Y, int ldc, const float* bias, int relu, int splits, int* err, void* stream);
 
+/* 3x3 "same" convolution as an implicit GEMM (no col matrix in memory): D = col(X) Wt^T with
+ * X NHWC BF16 [B*H*W][C] (C a multiple of 8), col as for unet_im2col with Kp = 9C, Wt [Cout][ldw]
+ * BF16 (ldw >= 9C, multiple of 8).  epilogue 0 (C = D, FP32), 2 (Y = bf16(act(D + bias))) or
+ * 3 (C = D + bias, FP32), row stride ldc.  Same results as unet_im2col + unet_gemm. */
+int unet_conv3x3(const void* X, int B, int H, int W, int C, const void* Wt, int ldw, int Cout, int epilogue,
+                 float* Cf, void* Y, int ldc, const float* bias, int relu, int* err, void* stream);
+
 /* Layer kernels.  Activations are NHWC ([pixels][channels], pixels ordered batch, row, column).
  * A 3x3 "same" convolution is the GEMM col(X) W^T with col(X)[m][(ky*3+kx)*C + c] =
  * X[b][y+ky-1][x+kx-1][c] (zero outside the canvas and for k >= 9C; Kp = padded K, multiple of 8). */

@@ -2,7 +2,8 @@
 
 Every product is the tcgen05 GEMM of ``unet_gemm``: a 3x3 "same" convolution is
 ``col(X) @ W^T`` with ``col`` built by ``unet_im2col`` (NHWC activations, K index
-``(ky*3+kx)*Cin + c`` padded to a multiple of 8).  Its gradients are ``dW^T = col(X)^T dZ``
+``(ky*3+kx)*Cin + c`` padded to a multiple of 8); in the forward pass, layers whose Cin is a
+multiple of 8 use ``unet_conv3x3``, the same GEMM gathering ``col`` on the fly.  Its gradients are ``dW^T = col(X)^T dZ``
 (split-K GEMM with FP32 atomics) and ``dX = col2im(dZ W)``.  Pooling (2x2 average), nearest
 upsampling, skip concatenation, ReLU backward, bias gradients, the masked MSE and Adam are the
 kernels of ``unet_ops.cu``.  torch only allocates device memory and orders work on its current
@@ -28,6 +29,7 @@ I = C.c_int
 
 _SIG = {
     "unet_gemm": [V, I, V, I, I, I, I, I, V, V, I, V, I, I, V, V],
+    "unet_conv3x3": [V, I, I, I, I, V, I, I, I, V, V, I, V, I, V, V],
     "unet_im2col": [V, I, I, I, I, I, V, V],
     "unet_col2im": [V, I, I, I, I, I, V, V],
     "unet_transpose_bf16": [V, I, I, I, V, I, V],
@@ -140,6 +142,7 @@ class UNet:
             off += (L.kp * L.cout + 63) // 64 * 64
         self.w_bf16 = torch.zeros(off, dtype=torch.bfloat16, device=device)
         self.t = 0
+        self.implicit = True   # forward convolutions with C % 8 == 0 as implicit GEMMs
         self.err = torch.zeros(1, dtype=torch.int32, device=device)
         self._ws = {}
         self.init_weights(seed)
@@ -249,10 +252,20 @@ class UNet:
         s = self._stream()
         B, H, W = ws["B"], ws["H"] >> lvl, ws["W"] >> lvl
         M = B * H * W
-        col = ws["col"]
-        _ok(K.unet_im2col(_p(X), B, H, W, L.cin, L.kp, _p(col), s), "im2col")
         wb = self.w_bf16.data_ptr() + 2 * L.off_wb
         bias = self.master.data_ptr() + 4 * L.off_b
+        if self.implicit and L.cin % 8 == 0 and L.kp == 9 * L.cin:
+            # implicit GEMM: the A operand is gathered from X, no col matrix in memory
+            if out_f32:
+                code = K.unet_conv3x3(_p(X), B, H, W, L.cin, wb, L.kp, L.cout, 3, _p(Y), None, L.cout, bias, 0,
+                                      _p(self.err), s)
+            else:
+                code = K.unet_conv3x3(_p(X), B, H, W, L.cin, wb, L.kp, L.cout, 2, None, _p(Y), L.cout, bias,
+                                      1 if L.relu else 0, _p(self.err), s)
+            _ok(code, f"conv3x3 {L.name}")
+            return
+        col = ws["col"]
+        _ok(K.unet_im2col(_p(X), B, H, W, L.cin, L.kp, _p(col), s), "im2col")
         if out_f32:
             code = K.unet_gemm(_p(col), L.kp, wb, L.kp, M, L.cout, L.kp, 3, _p(Y), None, L.cout, bias, 0, 1,
                                _p(self.err), s)

@@ -47,6 +47,10 @@ struct GemmArgs {
   int relu;
   int k_tiles_per_split; // split-K: blockIdx.z covers this many 64-wide K slabs
   int* err;              // set to 1 when an mbarrier wait times out
+  // implicit 3x3 convolution (k_gemm_tc<..., true>): A is the NHWC activation X [M = batch*H*W
+  // pixels][cH channels], row m of the virtual A is col(X)[m][(ky*3+kx)*cC + c] (zero outside the
+  // image), K = 9*cC with cC a multiple of 8
+  int cH, cW, cC;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -115,7 +119,28 @@ __device__ __forceinline__ void load_slab(uint32_t sbase, const __nv_bfloat16* G
   }
 }
 
-template <int BN, int EPI>
+// A slab of the virtual col(X) matrix: each 16-byte chunk is 8 channels of one tap of one pixel
+// (cC is a multiple of 8, so a chunk never straddles two taps), copied straight from X.
+__device__ __forceinline__ void load_slab_conv(uint32_t sbase, const GemmArgs& a, int r0, int k0) {
+  const int vecs = TC_BM * (TC_BK / 8);
+  for (int v = threadIdx.x; v < vecs; v += TC_THREADS) {
+    const int r = v >> 3, c = v & 7;
+    const int m = r0 + r, k = k0 + c * 8;
+    bool ok = m < a.M && k < a.K;
+    const __nv_bfloat16* src = a.A;
+    if (ok) {
+      const int tap = k / a.cC, ch = k - tap * a.cC;
+      const int ky = tap / 3, kx = tap - ky * 3;
+      const int x = m % a.cW, y = (m / a.cW) % a.cH, b = m / (a.cW * a.cH);
+      const int yy = y + ky - 1, xx = x + kx - 1;
+      ok = yy >= 0 && yy < a.cH && xx >= 0 && xx < a.cW;
+      if (ok) src = a.A + (((long long)b * a.cH + yy) * a.cW + xx) * a.cC + ch;
+    }
+    cp_async16(sbase + (uint32_t)(c * TC_BM * 16 + r * 16), src, ok);
+  }
+}
+
+template <int BN, int EPI, bool CONV = false>
 __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(GemmArgs a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   // layout: [TC_STAGES][A: 128 x 64][B: BN x 64] bf16, then one mbarrier per stage, the TMEM
@@ -155,7 +180,8 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(GemmArgs a) {
   // slab t of this split goes to stage t % S; cp.async group g holds slab g
   auto load_tile = [&](int t) {
     const uint32_t sa = smem_u32(smem + (t % S) * STAGE), sb = sa + A_BYTES;
-    load_slab(sa, a.A, a.lda, m0, a.M, (kt0 + t) * TC_BK, a.K, TC_BM);
+    if (CONV) load_slab_conv(sa, a, m0, (kt0 + t) * TC_BK);
+    else load_slab(sa, a.A, a.lda, m0, a.M, (kt0 + t) * TC_BK, a.K, TC_BM);
     load_slab(sb, a.B, a.ldb, n0, a.N, (kt0 + t) * TC_BK, a.K, BN);
   };
   for (int t = 0; t < S - 1; ++t) {

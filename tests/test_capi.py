@@ -1,5 +1,5 @@
-"""The C ABI: the library loads, exports every symbol include/acs.h declares, and its parameter
-block matches the oracle's layout.  No compute call is made here."""
+"""The C ABI: the library loads, exports every symbol the headers in include/ declare, and its
+parameter block matches the oracle's layout.  No compute call is made here."""
 import ctypes
 import os
 import re
@@ -7,10 +7,10 @@ import re
 from conftest import ROOT
 
 
-def _declared():
-    src = open(os.path.join(ROOT, "include", "acs.h")).read()
+def _declared(header="acs.h", prefix="acs_"):
+    src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(acs_[a-z0-9_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(" + prefix + r"[a-z0-9_]+)\s*\(", src)))
 
 
 def test_library_exports_every_declared_symbol(pkg):
@@ -21,6 +21,16 @@ def test_library_exports_every_declared_symbol(pkg):
     assert not missing, missing
     assert set(pkg.EXPORTED) <= set(names)
 
+
+def test_library_exports_every_network_kernel(pkg):
+    L = pkg.lib()
+    names = _declared("unet.h", "unet_")
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    from importlib import import_module
+    sig = import_module(pkg.__name__ + ".unet")._SIG
+    assert set(sig) == set(names)    # the Python binding declares every kernel
 
 def test_param_block_layout_matches_oracle(pkg, orc):
     a = [(n, t) for n, t in pkg.AcsParams._fields_]
