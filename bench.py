@@ -41,6 +41,9 @@ WORKLOADS = {
     "full-102": "full equation set (u, v, p, T, C), QUICK, porous block 30% (porosity 0.4, Da 1e-3, Cf 0.55), "
                 "Ri 1, Pr 0.7, Sc 1, Re 200, 102 x 102 stretched 2:1 channel, beta 1, dt 1e-3, residual 1e-6",
     "full-204": "as full-102 on a 204 x 204 mesh",
+    "large-1024x512": "the combined configuration's single large case: 1024 x 512 stretched 2:1 channel, two porous "
+                      "blocks (10% of the area each, porosity 0.4, Da 1e-3, Cf 0.55), Ri 1, Pr 0.7, Sc 1, scalars T "
+                      "and C, Re 400, QUICK, residual 1e-6",
     "plain-51": "plain method (u, v, p), first-order upwind, isothermal, no porous block, Re 100, 51 x 51 "
                 "stretched 2:1 channel, beta 1, dt 1e-3, residual 1e-6",
     "batch-256": "256 independent cases, nx, ny in {51,102,153,204}, Re U[50,500], Da logU[1e-5,1e-2], "
@@ -100,6 +103,10 @@ def _build_workload(pkg, name, arith, seed_offset=0):
     if name == "batch-256":
         items, _ = cfg.cfg_batch(256, seed=seed_offset, arith=a)
         return items, "full"
+    if name.startswith("large-"):
+        nx, ny = (int(v) for v in name.split("-")[1].split("x"))
+        prm, mesh, st, itc, _ = cfg.cfg_large(nx, ny, arith=a, seed=2 + seed_offset)
+        return [(prm, mesh, st, itc)], "full"
     if name.startswith("full-"):
         n = int(name.split("-")[1])
         prm, mesh, st, itc, _ = cfg.cfg_full(n, arith=a, seed=1 + seed_offset)
@@ -223,6 +230,7 @@ def run_product(args):
         tuned = {"threads": t, "ctas_per_sm": c_, "nodes_per_cta": n_, "staged": args.stage}
     elif args.arith == "fast" and args.engine == "cluster":
         tuned = import_module(pkg.__name__ + ".autotune").tune(pkg, items, use_cache=not args.retune)
+    eng_used = "graph" if (tuned or {}).get("engine") == 1 else args.engine
     batch = pkg.Batch([x[0] for x in items], [x[1] for x in items])
     batch.set_stream(stream.cuda_stream)
     batch.set_option(pkg.OPT_ENGINE, 0 if args.engine == "cluster" else 1)
@@ -272,7 +280,7 @@ def run_product(args):
     b_cu = BYTES_PER_CELL_UPDATE[kind]
     cell_updates = sum(iters[c].sum() * items[c][0].imax * items[c][0].jmax for c in range(n_cases))
     loop_gbs = b_cu * cell_updates / elapsed / 1e9
-    if args.engine == "cluster":
+    if eng_used == "cluster":
         # the persistent engine kernel is the whole loop: one launch per size class and step
         kern = "k_engine (persistent cluster engine, %s arithmetic)" % args.arith
         achieved = loop_gbs
@@ -282,12 +290,12 @@ def run_product(args):
     else:
         ms_u, nodes_u = batch.time_kernel(0, reps=50)
         b_node = U_KERNEL_BYTES[args.arith]
-        kern = "k_u_stage_exact (u-momentum stage, graph engine)"
+        kern = "k_u_stage_%s (u-momentum stage, graph engine)" % args.arith
         achieved = b_node * nodes_u / (ms_u * 1e-3) / 1e9
         per_launch = {"bytes_per_node": b_node, "nodes_per_launch": nodes_u, "ms_per_launch": ms_u}
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "engine_dram_bytes.json")
-    if args.engine == "cluster" and os.path.exists(tfile):
+    if eng_used == "cluster" and os.path.exists(tfile):
         with open(tfile) as f:
             bpcu = json.load(f).get(kind, {}).get("dram_bytes_per_cell_update")
         if bpcu:
@@ -348,7 +356,7 @@ def run_product(args):
                 "cases_per_gpu": n_cases,
                 "cells_per_gpu": cells,
                 "arith": args.arith,
-                "engine": args.engine,
+                "engine": "graph" if (tuned or {}).get("engine") == 1 else args.engine,
                 "staged": args.stage,
                 "launch_shape": tuned,
                 "pseudo_iterations_per_step_mean": total_iters / steps_done,
@@ -610,7 +618,7 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
                 "cases_per_gpu": n_cases,
                 "cells_per_gpu": cells * n_cases,
                 "arith": args.arith,
-                "engine": args.engine,
+                "engine": "graph" if (tuned or {}).get("engine") == 1 else args.engine,
                 "staged": args.stage,
                 "launch_shape": tuned,
                 "network": {"weights": os.path.relpath(args.weights, ROOT), "canvas": [H, W],
@@ -628,7 +636,9 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
             "cell_updates_per_s": cu_ws * world / el_ws,
             "roofline": {
                 "bound": "hbm",
-                "kernel": "k_engine (persistent cluster engine, %s arithmetic)" % args.arith,
+                "kernel": ("pseudo-time loop of the graph engine (per-stage kernels, %s arithmetic)" % args.arith
+                           if (tuned or {}).get("engine") == 1 else
+                           "k_engine (persistent cluster engine, %s arithmetic)" % args.arith),
                 "achieved": eng_gbs,
                 "peak": peak,
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst)" if peak_kind == "measured" else "fallback",

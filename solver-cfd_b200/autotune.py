@@ -3,7 +3,9 @@
 The engine's launch shape is set per batch by four knobs (include/acs.h, ACS_OPT_*):
 threads per CTA (256 or 512), resident CTAs per SM (1 or 2, 256 threads only), the target
 number of nodes per CTA, which fixes how many CTAs (1..16, one cluster) each case is split into,
-and whether each phase stages its stencil arrays in shared memory first.
+and whether each phase stages its stencil arrays in shared memory first.  The graph engine
+(per-stage kernels spread over the whole GPU, the better choice for a single large case) is
+timed as one more candidate.
 Besides powers of two, the candidates include the splits that make one wave of clusters fill the
 SMs (n_cases x K ~ SMs x CTAs per SM).  The best choice depends on the case sizes and on how many
 cases share the GPU, so it is measured:
@@ -49,6 +51,7 @@ def apply(batch, pkg, cfg: dict) -> None:
     batch.set_option(pkg.OPT_NODES_PER_CTA, cfg["nodes_per_cta"])
     batch.set_option(pkg.OPT_L1_LOADS, 1)
     batch.set_option(pkg.OPT_STAGED, cfg.get("staged", 1))
+    batch.set_option(pkg.OPT_ENGINE, cfg.get("engine", 0))
 
 
 def _sm_count() -> int:
@@ -94,6 +97,8 @@ def tune(pkg, items, iters: int = 200, use_cache: bool = True, verbose: bool = F
                 for staged in ((0, 1) if per_sm == 1 else (0,)):
                     cands.append({"threads": threads, "ctas_per_sm": per_sm, "nodes_per_cta": nodes,
                                   "staged": staged})
+        # the graph engine (per-stage kernels over the whole GPU): wins for single large cases
+        cands.append({"threads": 512, "ctas_per_sm": 1, "nodes_per_cta": 4096, "staged": 0, "engine": 1})
         for cfg in cands:
             apply(batch, pkg, cfg)
             for c, x in enumerate(capped):
@@ -109,7 +114,7 @@ def tune(pkg, items, iters: int = 200, use_cache: bool = True, verbose: bool = F
     finally:
         batch.close()
     best = max(table, key=lambda r: r["cell_updates_per_s"])
-    best = {k: best[k] for k in ("threads", "ctas_per_sm", "nodes_per_cta", "staged")}
+    best = {k: best[k] for k in ("threads", "ctas_per_sm", "nodes_per_cta", "staged")} | {"engine": best.get("engine", 0)}
     with open(path, "w") as f:
         json.dump({"key": key, "iterations_per_candidate": iters, "best": best, "table": table}, f, indent=1)
     return best

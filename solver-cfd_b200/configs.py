@@ -171,3 +171,22 @@ def cfg_batch(n_cases=256, seed=0, sizes=(51, 102, 153, 204), **kw):
         args.update(kw)
         out.append(channel_case(q["nx"], q["ny"], **args))
     return out, 200
+
+
+def cfg_large(nx=1024, ny=512, **kw):
+    """The combined configuration's single large case: nx x ny stretched 2:1 channel with two
+    porous blocks (each 10 % of the area, centred at x = Lx/4 and 3Lx/4), porosity 0.4, Da 1e-3,
+    Cf 0.55, Ri 1, Pr 0.7, Sc 1, scalars T and C with inflow value 1, Re 400, QUICK, 1000
+    physical steps, seed 2.  Returns (params, mesh, state, itc, n_steps)."""
+    Lx, Ly = 2.0, 1.0
+    w, h = math.sqrt(0.1) * Lx, math.sqrt(0.1) * Ly
+
+    def box(cx):
+        return (cx - 0.5 * w, cx + 0.5 * w, 0.5 * (Ly - h), 0.5 * (Ly + h))
+
+    args = dict(seed=2, Re=400.0, scheme=SCHEME_QUICK, block=box(0.25 * Lx), block2=box(0.75 * Lx),
+                porosity=0.4, Da=1.0e-3, Cf=0.55, Ri=1.0, Pr=0.7, Sc=1.0, scalars=True, beta=1.0,
+                dt=1.0e-3, eps=1.0e-6)
+    args.update(kw)
+    prm, mesh, st, itc = channel_case(nx, ny, **args)
+    return prm, mesh, st, itc, 1000

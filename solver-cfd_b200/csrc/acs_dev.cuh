@@ -92,4 +92,26 @@ __device__ inline void atomic_max_nonneg(unsigned long long* slot, double v) {
   atomicMax(slot, (unsigned long long)__double_as_longlong(v));
 }
 
+// Block-wide max of non-negative values, then one atomic per block.
+__device__ inline void block_max_to(unsigned long long* slot, double v) {
+  __shared__ double red[32];
+  unsigned m = 0xffffffffu;
+  for (int o = 16; o > 0; o >>= 1) {
+    double w = __shfl_xor_sync(m, v, o);
+    v = (w > v || w != w) ? w : v;
+  }
+  int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  int nw = (blockDim.x * blockDim.y + 31) / 32;
+  if ((tid & 31) == 0) red[tid >> 5] = v;
+  __syncthreads();
+  if (tid < 32) {
+    v = tid < nw ? red[tid] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      double w = __shfl_xor_sync(m, v, o);
+      v = (w > v || w != w) ? w : v;
+    }
+    if (tid == 0 && v != 0.0) atomic_max_nonneg(slot, v);
+  }
+}
+
 }  // namespace acs

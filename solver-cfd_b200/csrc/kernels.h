@@ -11,6 +11,11 @@ void launch_u_stage_exact(int stage, const CaseDev*, CaseCtl*, const Tile*, int 
 void launch_v_stage_exact(int stage, const CaseDev*, CaseCtl*, const Tile*, int ntiles, cudaStream_t);
 void launch_s_stage_exact(bool is_c, int stage, const CaseDev*, CaseCtl*, const Tile*, int ntiles, cudaStream_t);
 void launch_p_exact(const CaseDev*, CaseCtl*, const Tile*, int ntiles, cudaStream_t);
+// FAST-arithmetic per-stage kernels (kernels_fast.cu), same launch structure
+void launch_u_stage_fast(int stage, const CaseDev*, CaseCtl*, const Tile*, int ntiles, cudaStream_t);
+void launch_v_stage_fast(int stage, const CaseDev*, CaseCtl*, const Tile*, int ntiles, cudaStream_t);
+void launch_s_stage_fast(bool is_c, int stage, const CaseDev*, CaseCtl*, const Tile*, int ntiles, cudaStream_t);
+void launch_p_fast(const CaseDev*, CaseCtl*, const Tile*, int ntiles, cudaStream_t);
 // boundary passes, one block per case (see kernels_exact.cu for `which`)
 void launch_bc_uv(const CaseDev*, const CaseCtl*, int ncases, int which, cudaStream_t);
 void launch_bc_cell(const CaseDev*, const CaseCtl*, int ncases, int which, cudaStream_t);

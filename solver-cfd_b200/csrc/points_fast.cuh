@@ -1,0 +1,169 @@
+// points_fast.cuh -- per-node residuals with the FAST arithmetic, shared by the persistent
+// cluster engine (engine_fast.cu) and the per-stage kernels of the graph engine
+// (kernels_fast.cu).
+//
+// Same discretisation as the reference, rearranged for fewer FP64 operations:
+//   * every division by a metric difference becomes a product with a reciprocal precomputed
+//     once per case in 1-D tables (MX per column i, MY per row j);
+//   * the QUICK / upwind coefficient sums  -ap*uP + sum(a_nb*u_nb)  are evaluated in the
+//     equivalent face-value form  fw*phi_w - fe*phi_e + fs*phi_s - fn*phi_n  plus the diffusive
+//     face differences (the identity is exact in real arithmetic);
+//   * porosity enters through a 1-byte mask and per-case constants (1/phi, phi/(Re Da),
+//     Cf/sqrt(phi Da)) instead of two FP64 fields;
+//   * solve_P's three stages with frozen RP collapse to pn = p + dtau*beta*RP;
+//   * products and sums may fuse (FMA).
+// Reference (OpenMp_Multicore/): RESU equations.f90:2-116, RESV :305-420, RESZ :723-765,
+// RESC :823-867, solve_P :607-665.
+#pragma once
+#include <cuda_runtime.h>
+#include "acs_dev.cuh"
+
+namespace acs {
+
+// per-column table MX[i] = {x(i)-x(i-1), 1/(x(i)-x(i-1)), xm(i+1)-xm(i), 1/(xm(i+1)-xm(i))}
+// per-row    table MY[j] = {y(j)-y(j-1), 1/(y(j)-y(j-1)), ym(j+1)-ym(j), 1/(ym(j+1)-ym(j))}
+struct Met { double d, rd, dm, rdm; };
+
+__device__ __forceinline__ Met mx(const CaseDev& d, int i) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(d.mx) + 2 * i);
+  const double2 b = __ldg(reinterpret_cast<const double2*>(d.mx) + 2 * i + 1);
+  return {a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ Met my(const CaseDev& d, int j) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(d.my) + 2 * j);
+  const double2 b = __ldg(reinterpret_cast<const double2*>(d.my) + 2 * j + 1);
+  return {a.x, a.y, b.x, b.y};
+}
+// Loads of arrays written by other CTAs of the cluster: from L2 (.cg) or through L1 (.ca); the
+// cluster barrier's release/acquire pair orders the writes before the reads in both cases.
+struct LdL2 { static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldcg(a + q); } };
+struct LdL1 { static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldca(a + q); } };
+// Generic loads: the staged engine reads its stencil arrays from shared memory and the rest from
+// global memory written by this CTA or before the cluster barrier.
+struct LdGen { static __device__ __forceinline__ double ld(const double* a, long long q) { return a[q]; } };
+
+// QUICK face value seen from the face's upstream side (equations.f90:27-70 rearranged):
+// flux > 0 takes 0.75 of the upwind node, 0.375 of the downwind node, -0.125 of the far upwind.
+__device__ __forceinline__ double quick_face(double f, double up2, double up, double dn, double dn2) {
+  return f > 0.0 ? fma(0.75, up, fma(0.375, dn, -0.125 * up2)) : fma(0.75, dn, fma(0.375, up, -0.125 * dn2));
+}
+__device__ __forceinline__ double upw_face(double f, double up, double dn) { return f > 0.0 ? up : dn; }
+
+template <class L>
+struct PtFastT {
+  static __device__ __forceinline__ double ld(const double* a, long long q) { return L::ld(a, q); }
+  static __device__ __forceinline__ double F(const double* a, long long q) { return L::ld(a, q); }
+
+  // u-momentum residual RU at node (i,j)
+  static __device__ __forceinline__ double ru(const CaseDev& d, const double* um, const double* vm,
+                                              const double* p, int i, int j) {
+    const int P = d.pitch;
+    const long long q = lin(i, j, P);
+    const bool por = d.mask[q];
+    const double e = por ? d.phi : 1.0, ie = por ? d.fc[FC_IPHI] : 1.0;
+    const Met X = mx(d, i), Y = my(d, j), Yn = my(d, j + 1);
+    const double uP = F(um, q), uW = F(um, q - 1), uE = F(um, q + 1), uS = F(um, q - P), uN = F(um, q + P);
+    const double hx = 0.5 * X.d * ie, hy = 0.5 * Y.dm * ie;
+    const double fn = (F(vm, q + P) + F(vm, q + P - 1)) * hx;
+    const double fs = (F(vm, q) + F(vm, q - 1)) * hx;
+    const double fe = (uE + uP) * hy;
+    const double fw = (uP + uW) * hy;
+    const bool quick = d.scheme == 0 && j >= 3 && j <= d.ny - 2;
+    double conv;
+    if (quick) {
+      const double uWW = F(um, q - 2), uEE = F(um, q + 2), uSS = F(um, q - 2 * P), uNN = F(um, q + 2 * P);
+      conv = fw * quick_face(fw, uWW, uW, uP, uE) - fe * quick_face(fe, uW, uP, uE, uEE) +
+             fs * quick_face(fs, uSS, uS, uP, uN) - fn * quick_face(fn, uS, uP, uN, uNN);
+    } else {
+      conv = fw * upw_face(fw, uW, uP) - fe * upw_face(fe, uP, uE) + fs * upw_face(fs, uS, uP) - fn * upw_face(fn, uP, uN);
+    }
+    const double Xw = mx(d, i - 1).rdm;  // 1/(xm(i)-xm(i-1))
+    const double diff = e * d.fc[FC_IRE] *
+                        (X.d * (Yn.rd * (uN - uP) - Y.rd * (uP - uS)) + Y.dm * (X.rdm * (uE - uP) - Xw * (uP - uW)));
+    double r = X.rd * Y.rd * (conv + diff) - e * (F(p, q) - F(p, q - 1)) * X.rd;
+    if (d.flags & F_BART) {
+      const double dudxdx = Y.dm * (uE - uP) * X.rdm - Y.dm * (uP - uW) * Xw;
+      const double dxdvdy = Y.dm * (F(vm, q + P) - F(vm, q)) * Y.rdm - Y.dm * (F(vm, q + P - 1) - F(vm, q - 1)) * Y.rdm;
+      r += d.b_art * (dudxdx + dxdvdy);
+    }
+    if (por) {
+      const double vP = F(vm, q);
+      r -= e * uP * (d.fc[FC_IREDA] + d.fc[FC_CFS] * sqrt(fma(uP, uP, vP * vP)));
+    }
+    return r - d.g * e;
+  }
+
+  // v-momentum residual RV at node (i,j)
+  static __device__ __forceinline__ double rv(const CaseDev& d, const double* um, const double* vm,
+                                              const double* p, const double* T, int i, int j) {
+    const int P = d.pitch;
+    const long long q = lin(i, j, P);
+    const bool por = d.mask[q];
+    const double e = por ? d.phi : 1.0, ie = por ? d.fc[FC_IPHI] : 1.0;
+    const Met X = mx(d, i), Xe = mx(d, i + 1), Y = my(d, j), Ys = my(d, j - 1);
+    const double vP = F(vm, q), vW = F(vm, q - 1), vE = F(vm, q + 1), vS = F(vm, q - P), vN = F(vm, q + P);
+    const double hx = 0.5 * X.dm * ie, hy = 0.5 * Y.d * ie;
+    const double fn = (vP + vN) * hx;
+    const double fs = (vP + vS) * hx;
+    const double fe = (F(um, q + 1) + F(um, q + 1 - P)) * hy;
+    const double fw = (F(um, q) + F(um, q - P)) * hy;
+    const bool quick = d.scheme == 0 && i >= 3 && i <= d.nx - 2;
+    double conv;
+    if (quick) {
+      const double vWW = F(vm, q - 2), vEE = F(vm, q + 2), vSS = F(vm, q - 2 * P), vNN = F(vm, q + 2 * P);
+      conv = fw * quick_face(fw, vWW, vW, vP, vE) - fe * quick_face(fe, vW, vP, vE, vEE) +
+             fs * quick_face(fs, vSS, vS, vP, vN) - fn * quick_face(fn, vS, vP, vN, vNN);
+    } else {
+      conv = fw * upw_face(fw, vW, vP) - fe * upw_face(fe, vP, vE) + fs * upw_face(fs, vS, vP) - fn * upw_face(fn, vP, vN);
+    }
+    const double diff = e * d.fc[FC_IRE] *
+                        (X.dm * (Y.rdm * (vN - vP) - Ys.rdm * (vP - vS)) + Y.d * (Xe.rd * (vE - vP) - X.rd * (vP - vW)));
+    double r = X.rd * Y.rd * (conv + diff) - e * (F(p, q) - F(p, q - P)) * Y.rd;
+    if (d.flags & F_BART) {
+      const double dvdydy = X.dm * (vN - vP) * Y.rdm - X.dm * (vP - vS) * Ys.rdm;
+      const double dydudx = X.dm * (F(um, q + 1) - F(um, q)) * X.rdm - X.dm * (F(um, q + 1 - P) - F(um, q - P)) * X.rdm;
+      r += d.b_art * (dydudx + dvdydy);
+    }
+    if (d.flags & F_BUOY) r += d.InvFr2 * (1.0 - 2.0 / (F(T, q) + F(T, q - P)));
+    if (por) {
+      const double uP = F(um, q);
+      r -= e * vP * (d.fc[FC_IREDA] + d.fc[FC_CFS] * sqrt(fma(uP, uP, vP * vP)));
+    }
+    return r;
+  }
+
+  // RESZ (IS_C = false, diffusion 1/Pe) / RESC (IS_C = true, diffusion 1/(Re Sc))
+  template <bool IS_C>
+  static __device__ __forceinline__ double rs(const CaseDev& d, const double* un, const double* vn,
+                                              const double* z, int i, int j) {
+    const int P = d.pitch;
+    const long long q = lin(i, j, P);
+    const bool por = d.mask[q];
+    const Met X = mx(d, i), Xe = mx(d, i + 1), Y = my(d, j), Yn = my(d, j + 1);
+    const double zp = F(z, q), ze = F(z, q + 1), zw = F(z, q - 1), zn = F(z, q + P), zs = F(z, q - P);
+    const double conv = 0.5 * (Y.dm * ((ze + zp) * F(un, q + 1) - (zw + zp) * F(un, q)) +
+                               X.dm * ((zn + zp) * F(vn, q + P) - (zs + zp) * F(vn, q)));
+    const double k = IS_C ? d.fc[FC_IRESC] : d.fc[FC_IPE];
+    const double diff = k * (Y.dm * (Xe.rd * (ze - zp) - X.rd * (zp - zw)) + X.dm * (Yn.rd * (zn - zp) - Y.rd * (zp - zs)));
+    const double icap = por ? d.fc[FC_IPHI] : 1.0;
+    const double s = IS_C ? diff - conv * icap : (diff - (por ? 0.0 : conv)) * icap;
+    return X.rdm * Y.rdm * s;
+  }
+
+  // solve_P at one node: with RP frozen the three stages give pn = p + dtau*beta*RP
+  static __device__ __forceinline__ double p_update(const CaseDev& d, const double* p, const double* un,
+                                                    const double* vn, int i, int j, double* r) {
+    const int P = d.pitch;
+    const long long q = lin(i, j, P);
+    const Met X = mx(d, i), Y = my(d, j);
+    double RP = -((F(un, q + 1) - F(un, q)) * Y.dm + (F(vn, q + P) - F(vn, q)) * X.dm);
+    if (d.continuity == 1) RP *= X.rdm * Y.rdm;
+    *r = d.fc[FC_DTB] * RP;
+    return F(p, q) + *r;
+  }
+};
+
+// Read-only loads: in a per-stage kernel no array it reads is written during the launch.
+struct LdRO { static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldg(a + q); } };
+
+}  // namespace acs

@@ -464,7 +464,7 @@ int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch**
 // solve_U: three stages, each followed by bcUV(stage array, vm_tau) (equations.f90:259-296)
 void seq_u(Batch& b) {
   for (int s = 1; s <= 3; ++s) {
-    launch_u_stage_exact(s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
+    (b.use_fast ? launch_u_stage_fast : launch_u_stage_exact)(s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
     launch_bc_uv(b.dc, b.dk, b.n, s - 1, b.stream);
   }
   b.launches += 6;
@@ -473,7 +473,7 @@ void seq_u(Batch& b) {
 // solve_V: three stages, each followed by bcUV(um_tau, stage array) (equations.f90:561-598)
 void seq_v(Batch& b) {
   for (int s = 1; s <= 3; ++s) {
-    launch_v_stage_exact(s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
+    (b.use_fast ? launch_v_stage_fast : launch_v_stage_exact)(s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
     launch_bc_uv(b.dc, b.dk, b.n, 3 + s - 1, b.stream);
   }
   b.launches += 6;
@@ -481,7 +481,7 @@ void seq_v(Batch& b) {
 
 // solve_P: the stages fuse pointwise; the intermediate bcP(pi) never reaches the interior
 void seq_p(Batch& b) {
-  launch_p_exact(b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
+  (b.use_fast ? launch_p_fast : launch_p_exact)(b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
   launch_bc_cell(b.dc, b.dk, b.n, 0, b.stream);
   b.launches += 2;
 }
@@ -490,7 +490,7 @@ void seq_p(Batch& b) {
 void seq_s(Batch& b, bool is_c) {
   const int w0 = is_c ? 4 : 1;
   for (int s = 1; s <= 3; ++s) {
-    launch_s_stage_exact(is_c, s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
+    (b.use_fast ? launch_s_stage_fast : launch_s_stage_exact)(is_c, s, b.dc, b.dk, b.dtiles, b.ntiles, b.stream);
     launch_bc_cell(b.dc, b.dk, b.n, w0 + s - 1, b.stream);
   }
   b.launches += 6;
@@ -499,11 +499,11 @@ void seq_s(Batch& b, bool is_c) {
 // one launch of the timed kernel (acs_batch_time_kernel)
 void launch_timed_kernel(Batch& b, int kernel) {
   switch (kernel) {
-    case 0: launch_u_stage_exact(1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
-    case 1: launch_v_stage_exact(1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
-    case 2: launch_p_exact(b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
-    case 3: launch_s_stage_exact(false, 1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
-    case 4: launch_s_stage_exact(true, 1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
+    case 0: (b.use_fast ? launch_u_stage_fast : launch_u_stage_exact)(1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
+    case 1: (b.use_fast ? launch_v_stage_fast : launch_v_stage_exact)(1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
+    case 2: (b.use_fast ? launch_p_fast : launch_p_exact)(b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
+    case 3: (b.use_fast ? launch_s_stage_fast : launch_s_stage_exact)(false, 1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
+    case 4: (b.use_fast ? launch_s_stage_fast : launch_s_stage_exact)(true, 1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
   }
 }
 

@@ -193,9 +193,10 @@ def test_reference_run_51x84_matches_golden(gpu):
     assert int(it_g.sum()) == 314712
 
 
-def _fast_compare(pkg, orc, prm, mesh, st, itc, nsteps, tol=1e-10, l1=0, nodes_per_cta=None):
+def _fast_compare(pkg, orc, prm, mesh, st, itc, nsteps, tol=1e-10, l1=0, nodes_per_cta=None, engine=0):
     from dataclasses import replace
     g = pkg.Case(replace(prm, arith=pkg.ARITH_FAST), mesh)
+    g.set_option(pkg.OPT_ENGINE, engine)
     g.set_option(pkg.OPT_L1_LOADS, l1)
     if nodes_per_cta:
         g.set_option(pkg.OPT_NODES_PER_CTA, nodes_per_cta)
@@ -230,3 +231,43 @@ def test_fast_engine_channel_full_physics(gpu, orc, l1):
                                           block=cfg.centred_block(2, 1, 0.3), porosity=0.45, Da=1e-3,
                                           Cf=0.55, Ri=1.0, scalars=True, eps=1e-5, itc_max=60000)
     _fast_compare(gpu, orc, prm, mesh, st, itc, 3, l1=l1, nodes_per_cta=64)
+
+
+def test_fast_graph_engine(gpu, orc):
+    """FAST arithmetic in the graph engine's per-stage kernels: the reference case and a
+    full-physics channel case, same iteration counts as the oracle, fields within 1e-10."""
+    prm, mesh, st, itc, _ = gpu.configs.reference_case(12, itc_max=20000)
+    _fast_compare(gpu, orc, prm, mesh, st, itc, 8, engine=1)
+    cfg = gpu.configs
+    prm, mesh, st, itc = cfg.channel_case(30, 22, seed=7, Re=120.0, scheme=gpu.SCHEME_QUICK,
+                                          block=cfg.centred_block(2, 1, 0.3), porosity=0.45, Da=1e-3,
+                                          Cf=0.55, Ri=1.0, scalars=True, eps=1e-5, itc_max=60000)
+    _fast_compare(gpu, orc, prm, mesh, st, itc, 3, engine=1)
+
+
+@ENGINES
+def test_large_case_fast(gpu, orc, engine):
+    """The 1024 x 512 case in FAST arithmetic on both engines: capped steps, fields within
+    1e-10 of the oracle."""
+    prm, mesh, st, itc, _ = gpu.configs.cfg_large(itc_max=25)
+    _fast_compare(gpu, orc, prm, mesh, st, itc, 2, engine=engine)
+
+
+@ENGINES
+def test_large_case_bit_exact(gpu, orc, engine):
+    """The combined configuration's single 1024 x 512 case (two porous blocks, full scalars),
+    the largest grid of the benchmark configurations: two physical steps capped at itc_max = 25
+    (so each ends on the itc_max path) on the GPU against the oracle, bit for bit."""
+    pkg = gpu
+    prm, mesh, st, itc, _ = pkg.configs.cfg_large(itc_max=25)
+    g = pkg.Case(prm, mesh)
+    g.set_option(pkg.OPT_ENGINE, engine)
+    g.set_state(st)
+    itc_g, it_g, er_g, status = g.physical_steps(2, itc)
+    out = g.get_state()
+    ost = fcopy(st)
+    itc_o, it_o, er_o = orc.OracleCase(prm, mesh).run(ost, 2, itc)
+    assert status == pkg.CASE_DONE
+    assert list(it_g) == list(it_o) == [24, 25]   # step 1 starts at itc = 1 (main.f90:77)
+    for k in ("um", "vm", "p", "pn", "T", "C", "um_tau", "vm_tau", "T_tau", "C_tau"):
+        assert np.array_equal(out[k], ost[k]), k
