@@ -432,14 +432,31 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
     make, tuned = _tuned_batch(pkg, items, args, stream)
     l2 = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
 
+    # cost-aware cluster sizes: a batched step lasts as long as its slowest case, so each case gets
+    # CTAs in proportion to its pseudo-iterations of the previous step (cluster engine only)
+    # the total stays that of the tuned launch shape; only its distribution over the cases changes
+    slots = 0
+    if args.balance and tuned and tuned.get("engine", 0) == 0 and args.engine == "cluster":
+        npc = tuned["nodes_per_cta"]
+        for p, *_ in items:
+            k = -(-((p.imax + 1) * (p.jmax + 1)) // npc)
+            slots += max(1, min(k, 16, max(1, (p.jmax + 1) // 4)))
+
+    def balance(batch, its):
+        if slots and its is not None:
+            batch.balance_clusters(its, slots)
+
     A = make()
     wA = ws.WarmStart(A, H, W, net, norm)
     itc = np.array([x[3] for x in items], np.int32)
     prev_snap = None
+    it_last = None
     for w in range(args.warmup):
         if w == args.warmup - 1:
             prev_snap = [A.get_state(c) for c in range(n_cases)]
-        itc, _, _, _ = wA.step(itc, "learned")
+        itc, it_last, _, _ = wA.step(itc, "learned")
+        balance(A, it_last)
+    it_warm_last = None if it_last is None else np.array(it_last)
     torch.cuda.synchronize()
     snap = [A.get_state(c) for c in range(n_cases)]
     itc_snap = itc.copy()
@@ -477,6 +494,7 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
         itc, it, _, _ = batch.run(1, itc)
         e1.record(stream)
         e1.synchronize()
+        balance(batch, it[:, 0])
         return itc, it[:, 0], chosen, e0.elapsed_time(e1)
 
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
@@ -500,6 +518,7 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
     # plain GPU path, same steps from the same state: all K steps in one persistent launch, each
     # case advancing through its steps on its own
     B = make(snap)
+    balance(B, it_warm_last)
     if world > 1:
         dist.barrier()
     l2.fill_(-1.0)
@@ -516,6 +535,7 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
 
     # end to end through the C ABI with pinned host buffers: the same steps again
     C_ = make(prev_snap)
+    balance(C_, it_warm_last)
     wC = ws.WarmStart(C_, H, W, net, norm)
     wC.features()                       # history: the fields at the start of the last warm-up step
     host = []
@@ -625,6 +645,10 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
                             "trained_snapshots": meta.get("snapshots")},
                 "pseudo_iterations_per_step_mean": float(it_ws.mean()),
                 "starts_plain_extrap_learned": starts.round(3).tolist(),
+                "cluster_sizes": ("the launch shape's CTAs redistributed in proportion to each case's pseudo-"
+                                  f"iterations of the previous step, {slots} CTAs in total (plain run: by the "
+                                  "last warm-up step)") if slots
+                                 else "from the launch shape",
                 "l2": "flushed (256 MB write) before every timed step",
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             },
@@ -746,6 +770,8 @@ def main():
                     help="threads,ctas_per_sm,nodes_per_cta: skip the autotuner (profiling runs)")
     ap.add_argument("--stage", type=int, default=1, choices=[0, 1],
                     help="FAST engine: stage stencil arrays in shared memory (1) or read them from L1/L2 (0)")
+    ap.add_argument("--balance", type=int, default=1, choices=[0, 1],
+                    help="ws-* workloads: cluster sizes in proportion to each case's pseudo-iterations")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--max-iters", type=int, default=None,

@@ -206,6 +206,12 @@ enum acs_option {
                                 they fit in 220 KB; 0 reads them from L1/L2 */
 };
 int acs_batch_set_option(acs_batch* b, int option, long long value);
+/* Persistent cluster engine (no reference counterpart): the number of CTAs (1..16) of case
+ * case_id's cluster, overriding ACS_OPT_NODES_PER_CTA for that case; 0 restores the default.
+ * A batched step lasts as long as its slowest case, so a caller that knows which cases need the
+ * most pseudo-iterations (e.g. from the previous step) can give them more CTAs.  Still capped at
+ * (jmax+1)/4 (strips of at least 4 rows).  Results do not depend on it. */
+int acs_batch_set_cluster_size(acs_batch* b, int case_id, int ctas);
 int acs_set_option(acs_handle* h, int option, long long value);
 
 /* ---- learned warm start (no counterpart in the reference) ------------------------------------

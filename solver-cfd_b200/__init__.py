@@ -45,6 +45,7 @@ EXPORTED = (
     "acs_batch_run", "acs_batch_launch_count", "acs_launch_count", "acs_batch_time_kernel",
     "acs_batch_set_option", "acs_set_option", "acs_solve_u_static",
     "acs_batch_ws_enable", "acs_batch_ws_features", "acs_batch_ws_target", "acs_batch_set_start",
+    "acs_batch_set_cluster_size",
 )
 WS_IN, WS_OUT = 11, 8
 POLICY_BEST, POLICY_PREDICTED, POLICY_PLAIN = 0, 1, 2
@@ -128,6 +129,7 @@ def _declare(L):
     L.acs_batch_set_option.argtypes = [V, C.c_int, C.c_longlong]
     L.acs_set_option.argtypes = [V, C.c_int, C.c_longlong]
     L.acs_solve_u_static.argtypes = [C.POINTER(AcsParams), C.POINTER(AcsGrid), V, V, V, V, V, _D, V]
+    L.acs_batch_set_cluster_size.argtypes = [V, C.c_int, C.c_int]
     L.acs_batch_ws_enable.argtypes = [V, C.c_int, C.c_int]
     L.acs_batch_ws_features.argtypes = [V, V, V]
     L.acs_batch_ws_target.argtypes = [V, V, V]
@@ -413,6 +415,23 @@ class Batch:
         n = C.c_longlong(0)
         _check(lib().acs_batch_launch_count(self.h, C.byref(n)), "acs_batch_launch_count")
         return n.value
+
+    def set_cluster_size(self, c: int, ctas: int):
+        """CTAs of case c's cluster in the persistent engine (0: from OPT_NODES_PER_CTA)."""
+        _check(lib().acs_batch_set_cluster_size(self.h, c, ctas), "acs_batch_set_cluster_size")
+
+    def balance_clusters(self, iterations, slots: int, kmin: int = 1):
+        """Give each case CTAs in proportion to its pseudo-iteration count (e.g. of the last
+        step), within `slots` resident CTAs (SMs x CTAs per SM); returns the sizes."""
+        it = np.maximum(np.asarray(iterations, np.float64), 1.0)
+        k = np.clip(np.floor(slots * it / it.sum()), kmin, 16).astype(int)
+        while k.sum() > slots and (k > kmin).any():
+            k[np.argmax(np.where(k > kmin, k / it, -1))] -= 1
+        while k.sum() < slots and (k < 16).any():   # the rest to the most loaded CTAs
+            k[np.argmax(np.where(k < 16, it / k, -1))] += 1
+        for c in range(self.n):
+            self.set_cluster_size(c, int(k[c]))
+        return k
 
     # ---- learned warm start (device pointers: torch tensors' data_ptr()) -------------------
     def ws_enable(self, H: int, W: int):

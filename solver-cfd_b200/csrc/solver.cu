@@ -105,6 +105,7 @@ struct Batch {
   int ctas_per_sm = 1;   // FAST engine with 256 threads: 1 or 2 resident CTAs per SM
   int staged = 1;        // FAST engine: stage stencil arrays in shared memory where they fit
   int last_staged = 0;   // the last engine launch used the staged kernel
+  std::vector<int> cluster_override;  // per case: CTAs of its cluster (0 = from nodes_per_cta)
   int* d_cases = nullptr;
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> ev;
@@ -681,6 +682,7 @@ int cluster_size(const Batch& b, int c) {
   const CaseDev& d = b.hc[c];
   const long long nodes = (long long)(d.nx + 1) * (d.ny + 1);
   int K = (int)((nodes + b.nodes_per_cta - 1) / b.nodes_per_cta);
+  if (c < (int)b.cluster_override.size() && b.cluster_override[c] > 0) K = b.cluster_override[c];
   K = std::max(1, std::min(K, 16));
   K = std::min(K, std::max(1, (d.ny + 1) / 4));
   return K;
@@ -965,6 +967,16 @@ int acs_batch_time_kernel(acs_batch* h, int kernel, int reps, double* ms_mean, l
   r = acs::push_ctl(b);
   if (!r) CU(cudaStreamSynchronize(b.stream));
   return r;
+}
+
+int acs_batch_set_cluster_size(acs_batch* h, int c, int ctas) {
+  if (!h) return acs::fail(ACS_E_ARG, "null handle");
+  Batch& b = *h->b;
+  if (c < 0 || c >= b.n) return acs::fail(ACS_E_ARG, "case id out of range");
+  if (ctas < 0 || ctas > 16) return acs::fail(ACS_E_ARG, "cluster size must be 0..16");
+  if ((int)b.cluster_override.size() < b.n) b.cluster_override.assign(b.n, 0);
+  b.cluster_override[c] = ctas;
+  return ACS_OK;
 }
 
 int acs_batch_set_option(acs_batch* h, int option, long long value) {
