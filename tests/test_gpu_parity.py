@@ -123,6 +123,34 @@ def test_cluster_sizes_bit_exact(gpu, orc, nodes_per_cta):
     _loop_compare(gpu, orc, prm, mesh, st, itc, 2, 0, nodes_per_cta)
 
 
+def test_per_case_cluster_sizes_bit_exact(gpu):
+    """acs_batch_set_cluster_size changes how cases are split into CTAs, not the results: a batch
+    with per-case cluster sizes (1, 5, 16, and back to the default) equals the default batch."""
+    pkg = gpu
+    cfg = pkg.configs
+    cases = [cfg.channel_case(30 + 6 * k, 40, seed=11, case_id=k, Re=120.0 + 40 * k, scheme=pkg.SCHEME_QUICK,
+                              block=cfg.centred_block(2, 1, 0.3), porosity=0.5, Da=1e-2, Cf=0.55, Ri=0.5,
+                              scalars=True, itc_max=400) for k in range(4)]
+
+    def run(sizes):
+        b = pkg.Batch([c[0] for c in cases], [c[1] for c in cases])
+        for k, c in enumerate(cases):
+            b.set_state(k, c[2])
+            if sizes is not None:
+                b.set_cluster_size(k, sizes[k])
+        _, it, _, st = b.run(2, np.array([c[3] for c in cases], np.int32))
+        out = [b.get_state(k) for k in range(len(cases))]
+        b.close()
+        return it, st, out
+
+    it0, st0, out0 = run(None)
+    it1, st1, out1 = run([1, 5, 16, 0])
+    assert np.array_equal(it0, it1) and (st0 == pkg.CASE_DONE).all() and (st1 == pkg.CASE_DONE).all()
+    for a, b in zip(out0, out1):
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+
+
 @ENGINES
 def test_batch_equals_oracle_per_case(gpu, orc, engine):
     """Ragged batch (sizes, schemes, both boundary variants, converging and capped cases) in one
