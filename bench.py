@@ -435,12 +435,15 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
     # cost-aware cluster sizes: a batched step lasts as long as its slowest case, so each case gets
     # CTAs in proportion to its pseudo-iterations of the previous step (cluster engine only)
     # the total stays that of the tuned launch shape; only its distribution over the cases changes
+    # (--balance 2: the CTA slots of the whole GPU, SMs x CTAs per SM, instead)
     slots = 0
     if args.balance and tuned and tuned.get("engine", 0) == 0 and args.engine == "cluster":
         npc = tuned["nodes_per_cta"]
         for p, *_ in items:
             k = -(-((p.imax + 1) * (p.jmax + 1)) // npc)
             slots += max(1, min(k, 16, max(1, (p.jmax + 1) // 4)))
+        if args.balance == 2:
+            slots = max(slots, torch.cuda.get_device_properties(dev).multi_processor_count * tuned.get("ctas_per_sm", 1))
 
     def balance(batch, its):
         if slots and its is not None:
@@ -770,8 +773,9 @@ def main():
                     help="threads,ctas_per_sm,nodes_per_cta: skip the autotuner (profiling runs)")
     ap.add_argument("--stage", type=int, default=1, choices=[0, 1],
                     help="FAST engine: stage stencil arrays in shared memory (1) or read them from L1/L2 (0)")
-    ap.add_argument("--balance", type=int, default=1, choices=[0, 1],
-                    help="ws-* workloads: cluster sizes in proportion to each case's pseudo-iterations")
+    ap.add_argument("--balance", type=int, default=1, choices=[0, 1, 2],
+                    help="ws-* workloads: cluster sizes in proportion to each case's pseudo-iterations "
+                         "(1: within the tuned shape's CTA total, 2: within all CTA slots of the GPU)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--max-iters", type=int, default=None,
