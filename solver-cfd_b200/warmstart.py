@@ -27,7 +27,7 @@ import math
 
 import numpy as np
 
-from . import POLICY_BEST, START_LEARNED, WS_IN, WS_OUT, Batch
+from . import POLICY_BEST, WS_IN, WS_OUT, Batch
 from .unet import UNet, kernels as unet_kernels
 
 N_FIELDS = 5

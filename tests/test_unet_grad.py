@@ -8,7 +8,6 @@ Tolerances (stated here, used below):
   all parameters.  The product also rounds each layer's output gradient to BF16 before its two
   GEMMs (the oracle keeps it in FP32), which adds about 0.4 % noise per element.
 """
-import ctypes as C
 
 import numpy as np
 import pytest

@@ -2,7 +2,6 @@
 plain products, torch CPU autograd for the network's gradients)."""
 import ctypes as C
 
-import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
