@@ -1,0 +1,96 @@
+"""Host-side logic that needs no GPU: cost-aware cluster sizes, the autotuner's candidate splits,
+the warm start's canvas and normalisation, the network's layer table, the large configuration."""
+import numpy as np
+import pytest
+
+
+class _FakeBatch:
+    def __init__(self, n):
+        self.n = n
+        self.sizes = {}
+
+    def set_cluster_size(self, c, k):
+        self.sizes[c] = k
+
+
+def test_balance_clusters_keeps_total_and_favours_expensive_cases(pkg):
+    its = np.array([244654, 100000, 90000, 150000, 120000, 80000, 110000, 95000,
+                    130000, 105000, 90000, 85000, 99000, 140000, 160000, 102000])
+    f = _FakeBatch(len(its))
+    k = pkg.Batch.balance_clusters(f, its, 192)
+    assert k.sum() == 192 and k.min() >= 1 and k.max() <= 16
+    assert k[0] == k.max()                                   # the slowest case gets the most CTAs
+    assert (its / k).max() < (its / 12).max()                # the heaviest load per CTA goes down
+    assert f.sizes == {c: int(k[c]) for c in range(len(its))}
+    # more slots than 16 per case can use: everyone capped at 16
+    assert (pkg.Batch.balance_clusters(_FakeBatch(4), [1, 2, 3, 4], 1000) == 16).all()
+    # fewer slots than cases: one CTA each at least
+    assert (pkg.Batch.balance_clusters(_FakeBatch(5), [5, 1, 1, 1, 1], 3) >= 1).all()
+
+
+def test_autotune_fill_candidates(pkg):
+    from importlib import import_module
+    at = import_module(pkg.__name__ + ".autotune")
+    items, _ = pkg.configs.cfg_batch(16, seed=101, sizes=(153,))
+    c1 = at.fill_candidates(items, 148, 1)
+    nodes = 154 * 154
+    # 16 cases on 148 SMs: one wave at 148 // 16 = 9 CTAs per case, and the neighbours 8 and 10
+    assert sorted(-(-nodes // npc) for npc in c1) == [8, 9, 10]
+    assert at.fill_candidates(items, 0, 1) == []
+    assert at.signature(items) == at.signature(list(reversed(items)))
+
+
+def test_canvas_and_node_count(pkg):
+    from importlib import import_module
+    ws = import_module(pkg.__name__ + ".warmstart")
+    assert ws.canvas_for(153, 153) == (160, 160)
+    assert ws.canvas_for(24, 24) == (32, 32)
+    assert ws.canvas_for(100, 50) == (56, 104)
+    nx, ny = 7, 5
+    assert ws.valid_nodes(nx, ny) == (nx + 1) * ny + nx * (ny + 1) + 3 * nx * ny
+
+
+def test_normalizer_from_samples(pkg):
+    from importlib import import_module
+    ws = import_module(pkg.__name__ + ".warmstart")
+    rng = np.random.default_rng(0)
+    X = rng.standard_normal((3, 8, 8, 11)) * 4.0 + 2.0
+    T = rng.standard_normal((3, 8, 8, 8)) * 0.5
+    Wt = np.zeros((3, 8, 8, 8))
+    Wt[..., :5] = 1.0
+    Wt[:, 6:, :, :] = 0.0                                   # rows outside the case
+    n = ws.Normalizer.from_samples(X, T, Wt, device="cpu")
+    m = Wt[..., 0] > 0
+    assert np.allclose(n.in_shift.numpy()[0], X[..., 0][m].mean(), rtol=1e-5)
+    assert np.allclose(n.in_mul.numpy()[0], 1.0 / X[..., 0][m].std(), rtol=1e-5)
+    assert n.in_shift.numpy()[5] == 0.0 and n.in_mul.numpy()[5] == 1.0   # porous indicator untouched
+    osc = n.out_scale.numpy()
+    assert osc.shape == (16,) and np.allclose(osc[0], np.sqrt(np.mean(T[..., 0][m] ** 2)), rtol=1e-5)
+    assert (osc[5:8] == 1.0).all() and (osc[8:] == 1.0).all()   # padding channels, increment weights
+    d = n.to_dict()
+    assert set(d) == {"in_shift", "in_mul", "out_scale", "inc_weight", "smooth"}
+
+
+def test_layer_table_and_flops(pkg):
+    from importlib import import_module
+    un = import_module(pkg.__name__ + ".unet")
+    convs, n = un.layer_table()
+    names = [L.name for L in convs]
+    assert names[:2] == ["enc0a", "enc0b"] and names[-1] == "head" and len(convs) == 15
+    ends = 0
+    for L in convs:
+        assert L.off_w % 64 == 0 and L.off_w >= ends       # 16-byte aligned BF16 slices, no overlap
+        assert L.kp % 8 == 0 and L.kp >= 9 * L.cin
+        ends = L.off_b + L.cout
+    assert n >= ends and n == 1951808
+    # 2 * 9 * Cin * Cout * pixels summed over the layers (head at its 5 real channels)
+    assert un.conv_flops(160, 160) == 8493465600
+
+
+def test_large_configuration(pkg):
+    prm, mesh, st, itc, n = pkg.configs.cfg_large(64, 32)
+    assert (prm.imax, prm.jmax, n, itc) == (64, 32, 1000, 1)
+    flag = mesh["flag"] != 0
+    left, right = flag[:32].any(), flag[32:].any()
+    assert left and right and not flag[30:34].any()         # two separate blocks
+    assert prm.Re == 400.0 and prm.solve_scalars == 1
