@@ -1,7 +1,6 @@
 """Host-side logic that needs no GPU: cost-aware cluster sizes, the autotuner's candidate splits,
 the warm start's canvas and normalisation, the network's layer table, the large configuration."""
 import numpy as np
-import pytest
 
 
 class _FakeBatch:
