@@ -83,8 +83,11 @@ def tune(pkg, items, iters: int = 200, use_cache: bool = True, verbose: bool = F
     key = f"{_device_name(pkg)}-{signature(items)}"
     path = os.path.join(CACHE_DIR, key + ".json")
     if use_cache and os.path.exists(path):
-        with open(path) as f:
-            return json.load(f)["best"]
+        try:
+            with open(path) as f:
+                return json.load(f)["best"]
+        except (OSError, ValueError, KeyError):
+            pass  # unreadable cache entry: tune again
     capped = [(replace(p, itc_max=iters, arith=pkg.ARITH_FAST), m, s, itc) for p, m, s, itc in items]
     batch = pkg.Batch([x[0] for x in capped], [x[1] for x in capped])
     cells = np.array([p.imax * p.jmax for p, *_ in capped], float)
@@ -115,6 +118,10 @@ def tune(pkg, items, iters: int = 200, use_cache: bool = True, verbose: bool = F
         batch.close()
     best = max(table, key=lambda r: r["cell_updates_per_s"])
     best = {k: best[k] for k in ("threads", "ctas_per_sm", "nodes_per_cta", "staged")} | {"engine": best.get("engine", 0)}
-    with open(path, "w") as f:
+    # ranks of a multi-GPU run may tune the same workload at once: write a private file, then
+    # rename it into place (atomic), so a reader never sees a partial entry
+    tmp = f"{path}.{os.getpid()}.tmp"
+    with open(tmp, "w") as f:
         json.dump({"key": key, "iterations_per_candidate": iters, "best": best, "table": table}, f, indent=1)
+    os.replace(tmp, path)
     return best
