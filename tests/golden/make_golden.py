@@ -10,7 +10,12 @@ computed.  Sources (paths relative to the reference project):
   OpenMp_Multicore/data/grid_u.dat, grid_v.dat, mesh.dat  mesh of the same run
       (nonsymetric_mesh.f90:149-163): (xm(i), y(j)) and (x(i), ym(j)) pairs, i outer;
   OpenMp_Multicore/data/output_variables.dat             x, y, u, v, p, T, C (output.f90:10-15);
-  OpenMp_DoConcurrent/data/output_variables.dat          10 x 16 run of the do-concurrent build.
+  OpenMp_DoConcurrent/data/output_variables.dat, restart/restart{U,V,PTC}.dat, grid_u.dat,
+  grid_v.dat                                             10 x 16 run of the do-concurrent build.
+      Its mesh is that of nonsymetric_mesh.f90 at imax = 10; its fields were written by sources or
+      inputs other than the shipped ones (the porous block holds C = 0.05 and T relaxes from 0.05 towards
+      a bottom wall at 1, where the shipped initial.f90 and comum.f90 set both to 1), so only the
+      geometry and the file layout of that run pin anything.
 """
 import os
 import sys
@@ -41,8 +46,18 @@ def main(ref_root):
         xm=gu[:, 0, 0], y=gu[0, :, 1], x=gv[:, 0, 0], ym=gv[0, :, 1],
         output_variables=out)
     dc = os.path.join(ref_root, "OpenMp_DoConcurrent", "data")
-    out10 = read_numbers(os.path.join(dc, "output_variables.dat")).reshape(10, 16, 7)
-    np.savez_compressed(os.path.join(here, "doconcurrent_10x16.npz"), output_variables=out10)
+    nx, ny = 10, 16
+    out10 = read_numbers(os.path.join(dc, "output_variables.dat")).reshape(nx, ny, 7)
+    U = read_numbers(os.path.join(dc, "restart", "restartU.dat")).reshape(nx + 1, ny)
+    V = read_numbers(os.path.join(dc, "restart", "restartV.dat")).reshape(nx, ny + 1)
+    PTC = read_numbers(os.path.join(dc, "restart", "restartPTC.dat")).reshape(nx, ny, 3)
+    gu = read_numbers(os.path.join(dc, "grid_u.dat")).reshape(nx + 1, ny, 2)
+    gv = read_numbers(os.path.join(dc, "grid_v.dat")).reshape(nx, ny + 1, 2)
+    np.savez_compressed(
+        os.path.join(here, "doconcurrent_10x16.npz"),
+        imax=nx, jmax=ny, output_variables=out10,
+        um=U, vm=V, p=PTC[:, :, 0], T=PTC[:, :, 1], C=PTC[:, :, 2],
+        xm=gu[:, 0, 0], y=gu[0, :, 1], x=gv[:, 0, 0], ym=gv[0, :, 1])
     print("wrote fixtures to", here)
 
 

@@ -7,8 +7,8 @@ import pytest
 from conftest import GOLDEN
 
 
-def _golden():
-    return np.load(os.path.join(GOLDEN, "reference_51x84.npz"))
+def _golden(name="reference_51x84.npz"):
+    return np.load(os.path.join(GOLDEN, name))
 
 
 def test_reference_jmax(orc):
@@ -17,18 +17,22 @@ def test_reference_jmax(orc):
     assert orc.reference_jmax(10) == 16
 
 
-def test_mesh_matches_reference_grid_files(orc):
+@pytest.mark.parametrize("imax,name", [(51, "reference_51x84.npz"), (10, "doconcurrent_10x16.npz")])
+def test_mesh_matches_reference_grid_files(orc, imax, name):
     """x, y, xm, ym of nonsymetric_mesh.f90 against grid_u.dat / grid_v.dat (printed with 16
-    significant digits).  x is exact; the stretched half of y goes through tanh, whose last bits
-    differ between libm implementations, so y agrees to a few ulp (1e-14 relative)."""
-    g = _golden()
-    m = orc.mesh_reference(51)
+    significant digits) of the OpenMP build (imax 51) and of the do-concurrent build (imax 10).
+    The files hold 16 significant digits, and the stretched half of y goes through tanh, whose
+    last bits differ between libm implementations: every coordinate agrees to a few ulp of the
+    largest one (measured: at most 5.6e-16 of max |coordinate|)."""
+    g = _golden(name)
+    assert (int(g["imax"]), int(g["jmax"])) == (imax, orc.reference_jmax(imax))
+    m = orc.mesh_reference(imax)
     for k in ("x", "y", "xm", "ym"):
         ref = g[k]
         assert m[k].shape == ref.shape
-        np.testing.assert_allclose(m[k], ref, rtol=1e-14, atol=1e-15, err_msg=k)
-    # xm(1) = -(x(2)+x(1))/2 is the reference's quirk: +5.88 for x(1) = -6, x(2) = -5.76
-    assert m["xm"][0] == pytest.approx(5.88, abs=1e-14)
+        assert np.abs(m[k] - ref).max() <= 2e-15 * np.abs(ref).max(), k
+    # xm(1) = -(x(2)+x(1))/2 is the reference's quirk: positive, e.g. +5.88 for x(1) = -6, x(2) = -5.76
+    assert m["xm"][0] == pytest.approx(-0.5 * (g["x"][1] + g["x"][0]), abs=1e-14) and m["xm"][0] > 0
 
 
 def test_porous_flag_of_reference_mesh(orc):

@@ -1,8 +1,8 @@
 """Restart / output files in the reference driver's formats.
 
 Pins: the cell-centred velocities and the p, T, C columns of the reference's own
-OpenMp_Multicore/data/output_variables.dat (51 x 84, written by output.f90 from the state in
-data/restart/) against comp_mean of that state; exact write/read round trips; the reader order of
+output_variables.dat (OpenMp_Multicore 51 x 84 and OpenMp_DoConcurrent 10 x 16, written by
+output.f90 from the state in data/restart/) against comp_mean of that state; exact write/read round trips; the reader order of
 initial.f90's restart(); and, on the GPU, a checkpoint/resume through restart files that stays
 bit-identical to the oracle resuming from the same files.
 """
@@ -20,12 +20,15 @@ def rs(pkg):
     return importlib.import_module(pkg.__name__ + ".restart")
 
 
-def _golden():
-    return np.load(os.path.join(GOLDEN, "reference_51x84.npz"))
+def _golden(name="reference_51x84.npz"):
+    return np.load(os.path.join(GOLDEN, name))
 
 
-def test_comp_mean_matches_reference_output_file(rs):
-    g = _golden()
+@pytest.mark.parametrize("name", ["reference_51x84.npz", "doconcurrent_10x16.npz"])
+def test_comp_mean_matches_reference_output_file(rs, name):
+    """comp_mean of a run's restart files against the same run's output_variables.dat: the OpenMP
+    build at 51 x 84 and the do-concurrent build at 10 x 16."""
+    g = _golden(name)
     out = g["output_variables"]          # [imax][jmax][x, y, u, v, p, T, C], i outer (output.f90:12-18)
     u, v = rs.comp_mean(g["um"], g["vm"])
     for k, a in ((2, u), (3, v), (4, g["p"]), (5, g["T"]), (6, g["C"])):
