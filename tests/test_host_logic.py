@@ -1,5 +1,9 @@
 """Host-side logic that needs no GPU: cost-aware cluster sizes, the autotuner's candidate splits,
-the warm start's canvas and normalisation, the network's layer table, the large configuration."""
+choice and cache, the warm start's canvas and normalisation, the network's layer table, the
+large configuration."""
+import json
+import os
+
 import numpy as np
 
 
@@ -93,3 +97,55 @@ def test_large_configuration(pkg):
     left, right = flag[:32].any(), flag[32:].any()
     assert left and right and not flag[30:34].any()         # two separate blocks
     assert prm.Re == 400.0 and prm.solve_scalars == 1
+
+
+class _FakeTunePkg:
+    """Stands in for the library in the autotuner: a batch whose 'run' reports many pseudo-
+    iterations for one launch shape only, so that shape must win."""
+    ARITH_FAST = 1
+    OPT_THREADS, OPT_CTAS_PER_SM, OPT_NODES_PER_CTA, OPT_L1_LOADS, OPT_STAGED, OPT_ENGINE = range(1, 7)
+    WIN = {1: 512, 2: 1, 3: 1024, 5: 1, 6: 0}
+
+    def __init__(self):
+        self.batches = 0
+        pkg = self
+
+        class Batch:
+            def __init__(self, params, meshes):
+                pkg.batches += 1
+                self.n, self.opt = len(params), {}
+
+            def set_option(self, k, v):
+                self.opt[k] = v
+
+            def set_state(self, c, st):
+                pass
+
+            def run(self, steps, itc):
+                win = all(self.opt.get(k) == v for k, v in pkg.WIN.items())
+                return None, np.full((self.n, 1), 1000 if win else 10), None, None
+
+            def close(self):
+                pass
+
+        self.Batch = Batch
+
+
+def test_autotune_picks_fastest_and_caches_atomically(pkg, tmp_path, monkeypatch):
+    from importlib import import_module
+    at = import_module(pkg.__name__ + ".autotune")
+    monkeypatch.setattr(at, "CACHE_DIR", str(tmp_path))
+    items, _ = pkg.configs.cfg_batch(3, seed=5, sizes=(51,))
+    fake = _FakeTunePkg()
+    best = at.tune(fake, items, iters=20)
+    assert best == {"threads": 512, "ctas_per_sm": 1, "nodes_per_cta": 1024, "staged": 1, "engine": 0}
+    files = os.listdir(tmp_path)
+    assert len(files) == 1 and files[0].endswith(".json")          # no temporary file left behind
+    with open(os.path.join(tmp_path, files[0])) as f:
+        entry = json.load(f)
+    n_cand = sum(len(set(at.NODES)) * (2 if per_sm == 1 else 1) for _, per_sm in at.SHAPES) + 1
+    assert entry["best"] == best and len(entry["table"]) == n_cand   # no SMs visible: fixed candidates
+    assert at.tune(fake, items) == best and fake.batches == 1         # second call: from the cache
+    with open(os.path.join(tmp_path, files[0]), "w") as f:
+        f.write('{"key": "trunc')                                     # a partial entry is re-tuned
+    assert at.tune(fake, items, iters=20) == best and fake.batches == 2
