@@ -455,7 +455,7 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
     for w in range(args.warmup):
         if w == args.warmup - 1:
             prev_snap = [A.get_state(c) for c in range(n_cases)]
-        itc, it_last, _, _ = wA.step(itc, "learned")
+        itc, it_last, _, _ = wA.step(itc, "learned", warm_eps=args.warm_eps)
         balance(A, it_last)
     it_warm_last = None if it_last is None else np.array(it_last)
     torch.cuda.synchronize()
@@ -490,6 +490,9 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
         w.features()
         y = w.predict()
         chosen, _ = batch.set_start(y.data_ptr(), 8, w.norm.out_scale.data_ptr(), pkg.POLICY_BEST)
+        if args.warm_eps is not None:
+            for c in range(n_cases):
+                batch.set_tolerance(c, args.warm_eps if chosen[c] != pkg.START_PLAIN else batch.params[c].eps)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         itc, it, _, _ = batch.run(1, itc)
@@ -646,6 +649,7 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
                             "trained_snapshots": meta.get("snapshots")},
                 "pseudo_iterations_per_step_mean": float(it_ws.mean()),
                 "starts_plain_extrap_learned": starts.round(3).tolist(),
+                "warm_start_tolerance": args.warm_eps if args.warm_eps is not None else "each case's own (1e-6)",
                 "cluster_sizes": ("the launch shape's CTAs redistributed in proportion to each case's pseudo-"
                                   f"iterations of the previous step, {slots} CTAs in total (plain run: by the "
                                   "last warm-up step)") if slots
@@ -774,6 +778,9 @@ def main():
     ap.add_argument("--balance", type=int, default=1, choices=[0, 1, 2],
                     help="ws-* workloads: cluster sizes in proportion to each case's pseudo-iterations "
                          "(1: within the tuned shape's CTA total, 2: within all CTA slots of the GPU)")
+    ap.add_argument("--warm-eps", type=float, default=None,
+                    help="warm-start workload: residual tolerance of the warm-started cases of each step "
+                         "(default: every case keeps its own, 1e-6)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--max-iters", type=int, default=None,

@@ -212,6 +212,11 @@ int acs_batch_set_option(acs_batch* b, int option, long long value);
  * most pseudo-iterations (e.g. from the previous step) can give them more CTAs.  Still capped at
  * (jmax+1)/4 (strips of at least 4 rows).  Results do not depend on it. */
 int acs_batch_set_cluster_size(acs_batch* b, int case_id, int ctas);
+/* The pseudo-time residual tolerance of case case_id for the following steps: the `eps` of the
+ * exit test `error < eps` (main.f90:142; read from input/iterations.dat), initially the
+ * case's acs_params.eps.  A warm-start policy may iterate warm-started steps to a tighter
+ * tolerance than the plain ones.  eps must be positive and finite (ACS_E_ARG otherwise). */
+int acs_batch_set_tolerance(acs_batch* b, int case_id, double eps);
 int acs_set_option(acs_handle* h, int option, long long value);
 
 /* ---- learned warm start (no counterpart in the reference) ------------------------------------

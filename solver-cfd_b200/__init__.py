@@ -45,7 +45,7 @@ EXPORTED = (
     "acs_batch_run", "acs_batch_launch_count", "acs_launch_count", "acs_batch_time_kernel",
     "acs_batch_set_option", "acs_set_option", "acs_solve_u_static",
     "acs_batch_ws_enable", "acs_batch_ws_features", "acs_batch_ws_target", "acs_batch_set_start",
-    "acs_batch_set_cluster_size",
+    "acs_batch_set_cluster_size", "acs_batch_set_tolerance",
 )
 WS_IN, WS_OUT = 11, 8
 POLICY_BEST, POLICY_PREDICTED, POLICY_PLAIN = 0, 1, 2
@@ -130,6 +130,7 @@ def _declare(L):
     L.acs_set_option.argtypes = [V, C.c_int, C.c_longlong]
     L.acs_solve_u_static.argtypes = [C.POINTER(AcsParams), C.POINTER(AcsGrid), V, V, V, V, V, _D, V]
     L.acs_batch_set_cluster_size.argtypes = [V, C.c_int, C.c_int]
+    L.acs_batch_set_tolerance.argtypes = [V, C.c_int, C.c_double]
     L.acs_batch_ws_enable.argtypes = [V, C.c_int, C.c_int]
     L.acs_batch_ws_features.argtypes = [V, V, V]
     L.acs_batch_ws_target.argtypes = [V, V, V]
@@ -419,6 +420,11 @@ class Batch:
     def set_cluster_size(self, c: int, ctas: int):
         """CTAs of case c's cluster in the persistent engine (0: from OPT_NODES_PER_CTA)."""
         _check(lib().acs_batch_set_cluster_size(self.h, c, ctas), "acs_batch_set_cluster_size")
+
+    def set_tolerance(self, c: int, eps: float):
+        """Pseudo-time residual tolerance of case c for the following steps (initially its
+        params' eps)."""
+        _check(lib().acs_batch_set_tolerance(self.h, c, float(eps)), "acs_batch_set_tolerance")
 
     def balance_clusters(self, iterations, slots: int, kmin: int = 1):
         """Give each case CTAs in proportion to its pseudo-iteration count (e.g. of the last

@@ -979,6 +979,19 @@ int acs_batch_set_cluster_size(acs_batch* h, int c, int ctas) {
   return ACS_OK;
 }
 
+int acs_batch_set_tolerance(acs_batch* h, int c, double eps) {
+  if (!h) return acs::fail(ACS_E_ARG, "null handle");
+  Batch& b = *h->b;
+  if (c < 0 || c >= b.n) return acs::fail(ACS_E_ARG, "case id out of range");
+  if (!(eps > 0.0) || !std::isfinite(eps)) return acs::fail(ACS_E_ARG, "tolerance must be positive and finite");
+  b.prm[c].eps = eps;
+  b.hc[c].eps = eps;
+  // stream-ordered: launches already queued keep the old value, the next ones see the new one
+  CU(cudaMemcpyAsync(&b.dc[c].eps, &b.hc[c].eps, sizeof(double), cudaMemcpyHostToDevice, b.stream));
+  CU(cudaStreamSynchronize(b.stream));
+  return ACS_OK;
+}
+
 int acs_batch_set_option(acs_batch* h, int option, long long value) {
   if (!h) return acs::fail(ACS_E_ARG, "null handle");
   Batch& b = *h->b;

@@ -27,7 +27,7 @@ import math
 
 import numpy as np
 
-from . import POLICY_BEST, WS_IN, WS_OUT, Batch
+from . import POLICY_BEST, START_PLAIN, WS_IN, WS_OUT, Batch
 from .unet import UNet, kernels as unet_kernels
 
 N_FIELDS = 5
@@ -148,9 +148,11 @@ class WarmStart:
             src = dst
         return src
 
-    def step(self, itc, mode: str = "learned"):
+    def step(self, itc, mode: str = "learned", warm_eps: float | None = None):
         """One physical step of every case.  mode: "plain" (the reference's start), "extrap"
         (best of plain and extrapolated) or "learned" (best of plain, extrapolated and learned).
+        warm_eps: residual tolerance for the cases whose chosen start is not the plain one (the
+        others keep their params' eps); None keeps every case's own tolerance.
         Returns (itc, iters[n], chosen[n], res0[n,3])."""
         chosen = np.zeros(self.n, np.int32)
         res0 = np.full((self.n, 3), np.nan)
@@ -161,6 +163,9 @@ class WarmStart:
                 chosen, res0 = self.b.set_start(y.data_ptr(), WS_OUT, self.norm.out_scale.data_ptr(), POLICY_BEST)
             else:
                 chosen, res0 = self.b.set_start(None, WS_OUT, None, POLICY_BEST)
+        if warm_eps is not None:
+            for c in range(self.n):
+                self.b.set_tolerance(c, warm_eps if chosen[c] != START_PLAIN else self.b.params[c].eps)
         itc, iters, err, st = self.b.run(1, itc)
         return itc, iters[:, 0], chosen, res0
 

@@ -152,6 +152,44 @@ def test_per_case_cluster_sizes_bit_exact(gpu):
 
 
 @ENGINES
+def test_per_case_tolerance_bit_exact(gpu, orc, engine):
+    """acs_batch_set_tolerance between steps: each case equals an oracle run that switches to the
+    same tolerance after the first step (a tighter one, a looser one, an unchanged one)."""
+    from dataclasses import replace
+    cfg = gpu.configs
+    items = [cfg.reference_case(n, itc_max=6000, scheme=s)[:4]
+             for n, s in ((12, gpu.SCHEME_QUICK), (14, gpu.SCHEME_UPWIND), (16, gpu.SCHEME_QUICK))]
+    new_eps = [items[0][0].eps / 5, items[1][0].eps * 5, items[2][0].eps]
+    b = gpu.Batch([x[0] for x in items], [x[1] for x in items])
+    b.set_option(gpu.OPT_ENGINE, engine)
+    for c, x in enumerate(items):
+        b.set_state(c, x[2])
+    itc_g, it1, _, _ = b.run(1, [x[3] for x in items])
+    for c in range(3):
+        b.set_tolerance(c, new_eps[c])
+    itc_g, it2, _, st_g = b.run(2, itc_g)
+    assert (st_g == gpu.CASE_DONE).all()
+    for c, (prm, mesh, st, itc) in enumerate(items):
+        ost = fcopy(st)
+        itc_o, it_o1, _ = orc.OracleCase(prm, mesh).run(ost, 1, itc)
+        itc_o, it_o2, _ = orc.OracleCase(replace(prm, eps=new_eps[c]), mesh).run(ost, 2, itc_o)
+        assert list(it1[c]) == list(it_o1) and list(it2[c]) == list(it_o2) and itc_g[c] == itc_o, c
+        out = b.get_state(c)
+        for k in gpu.FIELDS:
+            assert np.array_equal(mask_dead(k, out[k], prm.bc), mask_dead(k, ost[k], prm.bc)), (c, k)
+        if c < 2:   # the change is visible: the case's own tolerance gives other counts
+            ref = fcopy(st)
+            _, it_ref, _ = orc.OracleCase(prm, mesh).run(ref, 3, itc)
+            assert (it_ref[1:].sum() < it2[c].sum()) == (new_eps[c] < prm.eps), c
+    for bad in (0.0, -1e-6, float("nan"), float("inf")):
+        with pytest.raises(gpu.AcsError):
+            b.set_tolerance(0, bad)
+    with pytest.raises(gpu.AcsError):
+        b.set_tolerance(3, 1e-6)
+    b.close()
+
+
+@ENGINES
 def test_batch_equals_oracle_per_case(gpu, orc, engine):
     """Ragged batch (sizes, schemes, both boundary variants, converging and capped cases) in one
     graph launch; each case bit-identical to its own oracle run."""
