@@ -69,4 +69,4 @@ def forward_loss(convs, levels, params: np.ndarray, X: np.ndarray, T: np.ndarray
     loss = (ww * (y - tt) ** 2).sum() * inv_norm
     loss.backward()
     g = flat_used.grad.detach().to(torch.float64).numpy()
-    return float(loss), y.detach().numpy(), g
+    return float(loss.detach()), y.detach().numpy(), g
