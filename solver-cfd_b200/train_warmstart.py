@@ -72,6 +72,8 @@ def main(argv=None):
     ap.add_argument("--modes", default="plain,extrap,learned")
     ap.add_argument("--out", default=os.path.join(HERE, "unet", "weights", "ws_153.npz"))
     ap.add_argument("--report", default=None)
+    ap.add_argument("--step-log", default=None,
+                    help="append one JSON line per case and evaluation step (iterations, error, start kept)")
     ap.add_argument("--load", default=None, help="skip generation and training; evaluate these weights")
     a = ap.parse_args(argv)
 
@@ -129,7 +131,11 @@ def main(argv=None):
 
     held = make_cases(pkg, a.n, a.eval_cases, a.seed + 1, arith)
     modes = tuple(a.modes.split(","))
-    out = ws.evaluate(lambda: make_batch(pkg, held), H, W, a.eval_steps, 1, net, norm, modes=modes, log=log)
+    step_log = ws.StepLog(a.step_log) if a.step_log else None
+    out = ws.evaluate(lambda: make_batch(pkg, held), H, W, a.eval_steps, 1, net, norm, modes=modes, log=log,
+                      step_log=step_log)
+    if step_log is not None:
+        step_log.close()
     res = {}
     for m in modes:
         it = out[m]["iters"]

@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import json
 import math
+import os
 
 import numpy as np
 
@@ -91,6 +92,50 @@ class Normalizer:
                 "inc_weight": self.out_scale.cpu().numpy()[WS_OUT:], "smooth": self.smooth}
 
 
+START_NAMES = ("plain", "extrap", "learned")
+STATUS_NAMES = ("running", "done", "failed")
+
+
+class StepLog:
+    """Per-step record of every case, one JSON object per line: the physical step, the case, its
+    pseudo-iterations, the loop's last error (max of the dtau-scaled u, v and p residuals, the
+    `error` of main.f90:139), the case status, and with a warm start the start that was kept and
+    the initial residual of each candidate (null where a candidate was not built)."""
+
+    def __init__(self, path_or_file, label: str | None = None):
+        self._own = isinstance(path_or_file, (str, os.PathLike))
+        self.f = open(path_or_file, "a") if self._own else path_or_file
+        self.label = label
+
+    @staticmethod
+    def records(step, iters, err, status=None, chosen=None, res0=None, label=None) -> list:
+        iters = np.asarray(iters).reshape(-1)
+        err = np.asarray(err, np.float64).reshape(-1)
+        out = []
+        for c in range(iters.size):
+            r = {"step": int(step), "case": c, "pseudo_iterations": int(iters[c]), "error": float(err[c])}
+            if label is not None:
+                r["run"] = label
+            if status is not None:
+                r["status"] = STATUS_NAMES[int(status[c])]
+            if chosen is not None:
+                r["start"] = START_NAMES[int(chosen[c])]
+            if res0 is not None:
+                r["initial_residual"] = {n: (None if not math.isfinite(v) else float(v))
+                                         for n, v in zip(START_NAMES, np.asarray(res0, np.float64)[c])}
+            out.append(r)
+        return out
+
+    def write(self, step, iters, err, status=None, chosen=None, res0=None):
+        for r in self.records(step, iters, err, status, chosen, res0, self.label):
+            self.f.write(json.dumps(r) + "\n")
+        self.f.flush()
+
+    def close(self):
+        if self._own:
+            self.f.close()
+
+
 class WarmStart:
     """Warm start of a Batch of cases drawn on one H x W canvas."""
 
@@ -102,6 +147,8 @@ class WarmStart:
         self.H, self.W = H, W
         self.net = net
         self.norm = norm or Normalizer.identity()
+        self.log: StepLog | None = None     # set to record every step as JSON lines
+        self.steps_done = 0
         batch.set_stream(torch.cuda.current_stream().cuda_stream)
         batch.ws_enable(H, W)
         f32 = dict(dtype=torch.float32, device="cuda")
@@ -167,6 +214,10 @@ class WarmStart:
             for c in range(self.n):
                 self.b.set_tolerance(c, warm_eps if chosen[c] != START_PLAIN else self.b.params[c].eps)
         itc, iters, err, st = self.b.run(1, itc)
+        if self.log is not None:
+            self.log.write(self.steps_done, iters[:, 0], err[:, 0], st,
+                           None if mode == "plain" else chosen, None if mode == "plain" else res0)
+        self.steps_done += 1
         return itc, iters[:, 0], chosen, res0
 
 
@@ -272,17 +323,20 @@ def load(path, device="cuda"):
 
 
 def evaluate(make_batch, H, W, n_steps, itc0, net=None, norm=None, modes=("plain", "extrap", "learned"),
-             log=None):
+             log=None, step_log: StepLog | None = None):
     """Run fresh copies of the same cases for n_steps in each mode.  Returns per mode the
     iterations [n, n_steps], the seconds per step (device time, CUDA events around the whole
     step: features, network, start selection and the pseudo-time loop), the fraction of cases
     per step that started plain / extrapolated / learned ("kept", [n_steps, 3]) and the final
-    fields."""
+    fields.  With step_log, every case's step is also recorded as a JSON line labelled by mode."""
     torch = __import__("torch")
     out = {}
     for mode in modes:
         b = make_batch()
         ws = WarmStart(b, H, W, net if mode == "learned" else None, norm)
+        if step_log is not None:
+            step_log.label = mode
+            ws.log = step_log
         itc = np.broadcast_to(np.asarray(itc0, np.int32), (b.n,)).copy()
         iters = np.zeros((b.n, n_steps), np.int64)
         kept = []

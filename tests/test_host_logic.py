@@ -149,3 +149,24 @@ def test_autotune_picks_fastest_and_caches_atomically(pkg, tmp_path, monkeypatch
     with open(os.path.join(tmp_path, files[0]), "w") as f:
         f.write('{"key": "trunc')                                     # a partial entry is re-tuned
     assert at.tune(fake, items, iters=20) == best and fake.batches == 2
+
+
+def test_step_log_records(pkg, tmp_path):
+    from importlib import import_module
+    ws = import_module(pkg.__name__ + ".warmstart")
+    path = tmp_path / "steps.jsonl"
+    log = ws.StepLog(str(path), label="learned")
+    res0 = np.array([[3e-3, 1e-3, 5e-4], [2e-3, 4e-3, np.nan]])
+    log.write(4, np.array([120, 7]), np.array([9.5e-7, 8.1e-7]), status=np.array([1, 2]),
+              chosen=np.array([2, 0]), res0=res0)
+    log.write(5, np.array([90, 1]), np.array([9.9e-7, np.nan]))       # a plain step: no start fields
+    log.close()
+    lines = [json.loads(x) for x in path.read_text().splitlines()]
+    assert len(lines) == 4
+    assert lines[0] == {"step": 4, "case": 0, "pseudo_iterations": 120, "error": 9.5e-7, "run": "learned",
+                        "status": "done", "start": "learned",
+                        "initial_residual": {"plain": 3e-3, "extrap": 1e-3, "learned": 5e-4}}
+    assert lines[1]["status"] == "failed" and lines[1]["start"] == "plain"
+    assert lines[1]["initial_residual"]["learned"] is None                 # candidate not built
+    assert lines[2]["step"] == 5 and "start" not in lines[2] and "status" not in lines[2]
+    assert lines[3]["error"] != lines[3]["error"]                           # NaN error kept as NaN
