@@ -47,7 +47,7 @@ WORKLOADS = {
     "batch-256": "256 independent cases, nx, ny in {51,102,153,204}, Re U[50,500], Da logU[1e-5,1e-2], "
                  "porosity U[0.3,0.9], Ri U[0,2], random block position, full equation set, QUICK",
 }
-BYTES_PER_CELL_UPDATE = {"full": 204, "plain": 112}   # fused-kernel model, see DESIGN.md
+BYTES_PER_CELL_UPDATE = {"full": 204, "plain": 112}   # each FP64 field read and written once per routine
 # per-node algorithmic bytes of the timed u-momentum kernel: reads u_in, um, um_tau, vm_tau, pn
 # (5 x 8 B) and the porous mask (1 B), writes u_out (8 B)
 U_KERNEL_BYTES = {"exact": 49, "fast": 41}
