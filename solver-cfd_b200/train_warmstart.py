@@ -14,7 +14,8 @@ with the grid fixed at n x n.  Steps:
    residual tolerance; pseudo-iterations per step, device seconds per step and the final
    fields' relative max-norm difference to the plain run are reported.
 
-Writes the weights (`--out`, .npz) and a JSON report (`--report`).
+Writes the weights (`--out`, .npz) and a JSON report (`--report`).  `--eval-only` skips steps
+1 and 2 and compares the starts that need no network; `--step-log` records every case's step.
 
     python solver-cfd_b200/train_warmstart.py --n 153 --train-cases 16 --gen-steps 30 \\
         --epochs 100 --eval-cases 4 --eval-steps 10
@@ -45,12 +46,15 @@ def make_cases(pkg, n, count, seed, arith):
     return cases
 
 
-def make_batch(pkg, cases, options=None):
+def make_batch(pkg, cases, options=None, launch_shape=None):
     b = pkg.Batch([c[0] for c in cases], [c[1] for c in cases])
     for k, c in enumerate(cases):
         b.set_state(k, c[2])
     for opt, val in (options or {}).items():
         b.set_option(opt, val)
+    if launch_shape is not None:
+        from importlib import import_module
+        import_module(pkg.__name__ + ".autotune").apply(b, pkg, launch_shape)
     return b
 
 
@@ -75,6 +79,10 @@ def main(argv=None):
     ap.add_argument("--step-log", default=None,
                     help="append one JSON line per case and evaluation step (iterations, error, start kept)")
     ap.add_argument("--load", default=None, help="skip generation and training; evaluate these weights")
+    ap.add_argument("--eval-only", action="store_true",
+                    help="no network: evaluate the plain and extrapolated starts only (--modes plain,extrap)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="evaluate with the autotuner's launch shape for the held-out cases")
     a = ap.parse_args(argv)
 
     import torch
@@ -88,7 +96,11 @@ def main(argv=None):
     log = lambda m: print(f"[{time.time() - t0:8.1f}s] {m}", flush=True)
     report = {"n": a.n, "canvas": [H, W], "args": vars(a)}
 
-    if a.load:
+    if a.eval_only:
+        if "learned" in a.modes.split(","):
+            raise SystemExit("--eval-only evaluates the starts that need no network: --modes plain,extrap")
+        net = norm = None
+    elif a.load:
         net, norm, H2, W2, meta = ws.load(a.load)
         assert (H2, W2) == (H, W)
         if a.smooth:
@@ -131,9 +143,14 @@ def main(argv=None):
 
     held = make_cases(pkg, a.n, a.eval_cases, a.seed + 1, arith)
     modes = tuple(a.modes.split(","))
+    shape = None
+    if a.autotune:
+        shape = import_module(pkg.__name__ + ".autotune").tune(pkg, held)
+        report["launch_shape"] = shape
+        log(f"launch shape {shape}")
     step_log = ws.StepLog(a.step_log) if a.step_log else None
-    out = ws.evaluate(lambda: make_batch(pkg, held), H, W, a.eval_steps, 1, net, norm, modes=modes, log=log,
-                      step_log=step_log)
+    out = ws.evaluate(lambda: make_batch(pkg, held, launch_shape=shape), H, W, a.eval_steps, 1, net, norm,
+                      modes=modes, log=log, step_log=step_log)
     if step_log is not None:
         step_log.close()
     res = {}

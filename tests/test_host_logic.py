@@ -5,6 +5,7 @@ import json
 import os
 
 import numpy as np
+import pytest
 
 
 class _FakeBatch:
@@ -170,3 +171,10 @@ def test_step_log_records(pkg, tmp_path):
     assert lines[1]["initial_residual"]["learned"] is None                 # candidate not built
     assert lines[2]["step"] == 5 and "start" not in lines[2] and "status" not in lines[2]
     assert lines[3]["error"] != lines[3]["error"]                           # NaN error kept as NaN
+
+
+def test_eval_only_refuses_the_learned_mode(pkg):
+    from importlib import import_module
+    tw = import_module(pkg.__name__ + ".train_warmstart")
+    with pytest.raises(SystemExit, match="plain,extrap"):
+        tw.main(["--eval-only", "--n", "24", "--modes", "plain,extrap,learned"])
