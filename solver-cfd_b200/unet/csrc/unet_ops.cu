@@ -207,7 +207,6 @@ __global__ void k_mse_grad(const float* __restrict__ out, const float* __restric
   const long long n = (long long)B * H * W * C;
   float s = 0.f;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(q % C);
     const long long p = q / C;
     const int x = (int)(p % W), y = (int)((p / W) % H);
     const float wq = w[q];
