@@ -448,11 +448,13 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
             batch.balance_clusters(its, slots)
 
     A = make()
-    wA = ws.WarmStart(A, H, W, net, norm)
+    wA = ws.WarmStart(A, H, W, net, norm, extrap_order=args.extrap_order)
     itc = np.array([x[3] for x in items], np.int32)
-    prev_snap = None
+    prev_snap = prev_snap2 = None
     it_last = None
     for w in range(args.warmup):
+        if w == args.warmup - 2 and args.extrap_order == 2:
+            prev_snap2 = [A.get_state(c) for c in range(n_cases)]
         if w == args.warmup - 1:
             prev_snap = [A.get_state(c) for c in range(n_cases)]
         itc, it_last, _, _ = wA.step(itc, "learned", warm_eps=args.warm_eps)
@@ -538,10 +540,14 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
     B.close()
 
     # end to end through the C ABI with pinned host buffers: the same steps again
-    C_ = make(prev_snap)
+    C_ = make(prev_snap2 if prev_snap2 is not None else prev_snap)
     balance(C_, it_warm_last)
-    wC = ws.WarmStart(C_, H, W, net, norm)
+    wC = ws.WarmStart(C_, H, W, net, norm, extrap_order=args.extrap_order)
     wC.features()                       # history: the fields at the start of the last warm-up step
+    if prev_snap2 is not None:          # (and of the one before, for the quadratic candidate)
+        for c in range(n_cases):
+            C_.set_state(c, prev_snap[c])
+        wC.features()
     host = []
     h2d = d2h = 0
     for c in range(n_cases):
@@ -650,6 +656,7 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
                 "pseudo_iterations_per_step_mean": float(it_ws.mean()),
                 "starts_plain_extrap_learned": starts.round(3).tolist(),
                 "warm_start_tolerance": args.warm_eps if args.warm_eps is not None else "each case's own (1e-6)",
+                "extrapolation_order": args.extrap_order,
                 "cluster_sizes": ("the launch shape's CTAs redistributed in proportion to each case's pseudo-"
                                   f"iterations of the previous step, {slots} CTAs in total (plain run: by the "
                                   "last warm-up step)") if slots
@@ -778,6 +785,8 @@ def main():
     ap.add_argument("--balance", type=int, default=1, choices=[0, 1, 2],
                     help="ws-* workloads: cluster sizes in proportion to each case's pseudo-iterations "
                          "(1: within the tuned shape's CTA total, 2: within all CTA slots of the GPU)")
+    ap.add_argument("--extrap-order", type=int, default=1, choices=[1, 2],
+                    help="warm-start workload: linear (1) or quadratic (2) extrapolated candidate")
     ap.add_argument("--warm-eps", type=float, default=None,
                     help="warm-start workload: residual tolerance of the warm-started cases of each step "
                          "(default: every case keeps its own, 1e-6)")

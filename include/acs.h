@@ -201,9 +201,13 @@ enum acs_option {
   ACS_OPT_L1_LOADS = 3,      /* FAST engine: 1 (default) reads cluster-written arrays through L1 */
   ACS_OPT_THREADS = 4,       /* FAST engine: threads per CTA, 256 or 512 (default) */
   ACS_OPT_CTAS_PER_SM = 5,   /* FAST engine, 256 threads: 2 caps registers so two CTAs share an SM */
-  ACS_OPT_STAGED = 6         /* FAST engine: 1 (default) copies each phase's stencil arrays (the
+  ACS_OPT_STAGED = 6,        /* FAST engine: 1 (default) copies each phase's stencil arrays (the
                                 CTA's rows plus two halo rows) into shared memory first, where
                                 they fit in 220 KB; 0 reads them from L1/L2 */
+  ACS_OPT_EXTRAP_ORDER = 7   /* warm start: the extrapolated candidate of acs_batch_set_start is
+                                x + inc (1, default) or x + (2 inc - inc_prev), the quadratic
+                                through the last three step starts (2; linear until three
+                                acs_batch_ws_features calls have given two increments) */
 };
 int acs_batch_set_option(acs_batch* b, int option, long long value);
 /* Persistent cluster engine (no reference counterpart): the number of CTAs (1..16) of case

@@ -112,6 +112,8 @@ struct Batch {
   // learned warm start (warmstart.cu): canvas size, per-case previous fields and increments
   int ws_H = 0, ws_W = 0;
   int ws_has_prev = 0;
+  int ws_calls = 0;   // feature calls since acs_batch_ws_enable (3 give two increments)
+  int ws_order = 1;   // ACS_OPT_EXTRAP_ORDER
   char* ws_pool = nullptr;
   WsCase* d_ws = nullptr;
   unsigned long long* d_ws_res = nullptr;
@@ -856,7 +858,7 @@ int acs_batch_ws_enable(acs_batch* h, int H, int W) {
   if (H <= 0 || W <= 0 || (long long)H * W > (1LL << 30)) return acs::fail(ACS_E_ARG, "bad canvas size");
   if (!b.ws_pool) {
     size_t bytes = 0;
-    for (int c = 0; c < b.n; ++c) bytes += 2 * acs::WS_FIELDS * acs::align_up(8 * b.hc[c].n_elems, 256);
+    for (int c = 0; c < b.n; ++c) bytes += 3 * acs::WS_FIELDS * acs::align_up(8 * b.hc[c].n_elems, 256);
     CU(cudaMalloc(&b.ws_pool, bytes));
     CU(cudaMemsetAsync(b.ws_pool, 0, bytes, b.stream));
     std::vector<acs::WsCase> hw(b.n);
@@ -865,6 +867,7 @@ int acs_batch_ws_enable(acs_batch* h, int H, int W) {
       for (int f = 0; f < acs::WS_FIELDS; ++f) {
         hw[c].prev[f] = (double*)q; q += acs::align_up(8 * b.hc[c].n_elems, 256);
         hw[c].inc[f] = (double*)q; q += acs::align_up(8 * b.hc[c].n_elems, 256);
+        hw[c].incp[f] = (double*)q; q += acs::align_up(8 * b.hc[c].n_elems, 256);
       }
     CU(cudaMalloc(&b.d_ws, sizeof(acs::WsCase) * b.n));
     CU(cudaMemcpyAsync(b.d_ws, hw.data(), sizeof(acs::WsCase) * b.n, cudaMemcpyHostToDevice, b.stream));
@@ -878,6 +881,7 @@ int acs_batch_ws_enable(acs_batch* h, int H, int W) {
   b.ws_H = H;
   b.ws_W = W;
   b.ws_has_prev = 0;
+  b.ws_calls = 0;
   return ACS_OK;
 }
 
@@ -889,6 +893,7 @@ int acs_batch_ws_features(acs_batch* h, float* X, float* inc_scale) {
                           b.stream);
   CU(cudaGetLastError());
   b.ws_has_prev = 1;
+  ++b.ws_calls;
   return ACS_OK;
 }
 
@@ -908,8 +913,10 @@ int acs_batch_set_start(acs_batch* h, const float* Y, int ldy, const float* scal
   if (!b.ws_pool) return acs::fail(ACS_E_STATE, "warm start not enabled");
   if (policy < 0 || policy > 2) return acs::fail(ACS_E_ARG, "policy must be 0, 1 or 2");
   if (Y && (!scale || ldy < acs::WS_FIELDS)) return acs::fail(ACS_E_ARG, "Y needs scale and ldy >= 5");
-  acs::launch_ws_start(b.dc, b.dk, b.d_ws, b.n, b.ws_H, b.ws_W, b.d_ws_sc, Y, ldy, scale, policy, b.d_ws_res,
-                       b.d_ws_choice, b.stream);
+  // the quadratic candidate needs two increments, i.e. three feature calls; before that, linear
+  const int order = (b.ws_order == 2 && b.ws_calls >= 3) ? 2 : 1;
+  acs::launch_ws_start(b.dc, b.dk, b.d_ws, b.n, b.ws_H, b.ws_W, b.d_ws_sc, Y, ldy, scale, policy, order,
+                       b.d_ws_res, b.d_ws_choice, b.stream);
   CU(cudaGetLastError());
   int r = acs::pull_ctl(b);  // the commit kernel set tau_dirty where the prediction was kept
   if (r) return r;
@@ -1017,6 +1024,10 @@ int acs_batch_set_option(acs_batch* h, int option, long long value) {
       return ACS_OK;
     case ACS_OPT_STAGED:
       b.staged = value ? 1 : 0;
+      return ACS_OK;
+    case ACS_OPT_EXTRAP_ORDER:
+      if (value != 1 && value != 2) return acs::fail(ACS_E_ARG, "extrapolation order must be 1 or 2");
+      b.ws_order = (int)value;
       return ACS_OK;
   }
   return acs::fail(ACS_E_ARG, "unknown option");

@@ -5,7 +5,8 @@
 // increment over the step just completed and s[f] its RMS over the case (per field), the
 // candidate starts of the next pseudo-time loop are
 //   plain:    the stale pseudo-iterate the reference starts from (main.f90:145-149 skipped),
-//   extrap:   x + inc,
+//   extrap:   x + inc, or with order 2 x + (2 inc - incp) (incp: the increment one step
+//             earlier; the quadratic through the starts of the last three steps),
 //   learned:  x + a[f] * inc + s[f] * scale[f] * Y     (Y = network output, a[f] = scale[8+f],
 //             normally 1; a field whose increment is not predictable can take 0 or 1 there),
 // each with the boundary passes applied.  The initial residual -- the dtau-scaled max-norm of
@@ -48,7 +49,7 @@ __device__ inline double* phys_field(const CaseDev& d, const CaseCtl& k, int f) 
   }
 }
 
-// per node: inc = x - prev, prev = x; per case and field the sum of inc^2 into ss[c*8 + f]
+// per node: incp = inc, inc = x - prev, prev = x; per case and field the sum of inc^2 into ss[c*8 + f]
 __global__ void __launch_bounds__(WT) k_ws_history(const CaseDev* __restrict__ dc, const CaseCtl* __restrict__ dk,
                                                    const WsCase* __restrict__ dw, int H, int W, int has_prev,
                                                    double* __restrict__ ss) {
@@ -70,6 +71,7 @@ __global__ void __launch_bounds__(WT) k_ws_history(const CaseDev* __restrict__ d
         if (in_field(d, f, i, j)) {
           const double a = phys_field(d, k, f)[n];
           const double di = has_prev ? a - w.prev[f][n] : 0.0;
+          w.incp[f][n] = w.inc[f][n];
           w.inc[f][n] = di;
           w.prev[f][n] = a;
           sq[f] = di * di;
@@ -152,10 +154,14 @@ __global__ void __launch_bounds__(WT) k_ws_target(const CaseDev* __restrict__ dc
   }
 }
 
-// extrapolated (yy null): x + inc; learned: x + scale[8+f] * inc + s[f] * scale[f] * Y
+// extrapolated (yy null): x + inc (order 1) or x + (2 inc - incp) (order 2);
+// learned: x + scale[8+f] * inc + s[f] * scale[f] * Y
 __device__ inline double start_value(const CaseDev& d, const CaseCtl& k, const WsCase& w, const double* sc,
-                                     const float* yy, const float* scale, int c, int f, long long n) {
-  if (!yy) return phys_field(d, k, f)[n] + w.inc[f][n];
+                                     const float* yy, const float* scale, int order, int c, int f, long long n) {
+  if (!yy) {
+    if (order == 2) return phys_field(d, k, f)[n] + (2.0 * w.inc[f][n] - w.incp[f][n]);
+    return phys_field(d, k, f)[n] + w.inc[f][n];
+  }
   const double corr = sc[c * WS_OUT + f] * (double)scale[f] * (double)yy[f];
   return phys_field(d, k, f)[n] + (double)scale[WS_OUT + f] * w.inc[f][n] + corr;
 }
@@ -164,7 +170,7 @@ __device__ inline double start_value(const CaseDev& d, const CaseCtl& k, const W
 __global__ void __launch_bounds__(WT) k_ws_candidate(const CaseDev* __restrict__ dc, const CaseCtl* __restrict__ dk,
                                                      const WsCase* __restrict__ dw, int H, int W,
                                                      const double* __restrict__ sc, const float* __restrict__ Y,
-                                                     int ldy, const float* __restrict__ scale) {
+                                                     int ldy, const float* __restrict__ scale, int order) {
   const int c = blockIdx.y;
   const int q = blockIdx.x * WT + threadIdx.x;
   if (q >= H * W) return;
@@ -176,7 +182,7 @@ __global__ void __launch_bounds__(WT) k_ws_candidate(const CaseDev* __restrict__
   const float* yy = Y ? Y + ((long long)c * H * W + q) * ldy : nullptr;
 #pragma unroll
   for (int f = 0; f < 3; ++f)
-    if (in_field(d, f, i, j)) d.S[f][n] = start_value(d, k, dw[c], sc, yy, scale, c, f, n);
+    if (in_field(d, f, i, j)) d.S[f][n] = start_value(d, k, dw[c], sc, yy, scale, order, c, f, n);
 }
 
 __global__ void k_ws_bc_candidate(const CaseDev* __restrict__ dc) {
@@ -249,7 +255,7 @@ __device__ inline int pick(int policy, bool have_y, const unsigned long long* r)
 __global__ void __launch_bounds__(WT) k_ws_commit(const CaseDev* __restrict__ dc, CaseCtl* __restrict__ dk,
                                                   const WsCase* __restrict__ dw, int H, int W,
                                                   const double* __restrict__ sc, const float* __restrict__ Y, int ldy,
-                                                  const float* __restrict__ scale, int policy,
+                                                  const float* __restrict__ scale, int policy, int order,
                                                   const unsigned long long* __restrict__ res, int* __restrict__ choice) {
   const int c = blockIdx.y;
   const int q = blockIdx.x * WT + threadIdx.x;
@@ -266,13 +272,13 @@ __global__ void __launch_bounds__(WT) k_ws_commit(const CaseDev* __restrict__ dc
   const long long n = lin(i, j, d.pitch);
   const float* yy = which == 2 ? Y + ((long long)c * H * W + q) * ldy : nullptr;
   const WsCase& w = dw[c];
-  if (in_field(d, 0, i, j)) d.U[k.ru[R_TAU]][n] = start_value(d, k, w, sc, yy, scale, c, 0, n);
-  if (in_field(d, 1, i, j)) d.V[k.rv[R_TAU]][n] = start_value(d, k, w, sc, yy, scale, c, 1, n);
+  if (in_field(d, 0, i, j)) d.U[k.ru[R_TAU]][n] = start_value(d, k, w, sc, yy, scale, order, c, 0, n);
+  if (in_field(d, 1, i, j)) d.V[k.rv[R_TAU]][n] = start_value(d, k, w, sc, yy, scale, order, c, 1, n);
   if (in_field(d, 2, i, j)) {
-    const double pv = start_value(d, k, w, sc, yy, scale, c, 2, n);
+    const double pv = start_value(d, k, w, sc, yy, scale, order, c, 2, n);
     if (k.scalars) {
-      d.T[k.rt[R_TAU]][n] = start_value(d, k, w, sc, yy, scale, c, 3, n);
-      d.C[k.rc[R_TAU]][n] = start_value(d, k, w, sc, yy, scale, c, 4, n);
+      d.T[k.rt[R_TAU]][n] = start_value(d, k, w, sc, yy, scale, order, c, 3, n);
+      d.C[k.rc[R_TAU]][n] = start_value(d, k, w, sc, yy, scale, order, c, 4, n);
     }
     // p and pn both hold the start (the reads above went through P[rp_read] first)
     d.P[0][n] = pv;
@@ -317,19 +323,19 @@ void launch_ws_target(const CaseDev* dc, const CaseCtl* dk, const WsCase* dw, in
 }
 
 void launch_ws_start(const CaseDev* dc, CaseCtl* dk, const WsCase* dw, int n, int H, int W, const double* sc,
-                     const float* Y, int ldy, const float* scale, int policy, unsigned long long* res, int* choice,
-                     cudaStream_t s) {
+                     const float* Y, int ldy, const float* scale, int policy, int order, unsigned long long* res,
+                     int* choice, cudaStream_t s) {
   cudaMemsetAsync(res, 0, sizeof(unsigned long long) * 3 * n, s);
   const dim3 g = canvas_grid(n, H, W);
-  k_ws_candidate<<<g, WT, 0, s>>>(dc, dk, dw, H, W, sc, nullptr, ldy, scale);
+  k_ws_candidate<<<g, WT, 0, s>>>(dc, dk, dw, H, W, sc, nullptr, ldy, scale, order);
   k_ws_bc_candidate<<<n, 128, 0, s>>>(dc);
   k_ws_probe<<<g, WT, 0, s>>>(dc, dk, H, W, 0, 1, res);
   if (Y) {
-    k_ws_candidate<<<g, WT, 0, s>>>(dc, dk, dw, H, W, sc, Y, ldy, scale);
+    k_ws_candidate<<<g, WT, 0, s>>>(dc, dk, dw, H, W, sc, Y, ldy, scale, order);
     k_ws_bc_candidate<<<n, 128, 0, s>>>(dc);
     k_ws_probe<<<g, WT, 0, s>>>(dc, dk, H, W, -1, 2, res);
   }
-  k_ws_commit<<<g, WT, 0, s>>>(dc, dk, dw, H, W, sc, Y, ldy, scale, policy, res, choice);
+  k_ws_commit<<<g, WT, 0, s>>>(dc, dk, dw, H, W, sc, Y, ldy, scale, policy, order, res, choice);
   k_ws_bc_commit<<<n, 128, 0, s>>>(dc, dk, choice);
 }
 

@@ -17,9 +17,10 @@ constexpr int WS_OUT = 8;        // 5 increment channels, padded to 8
 struct WsCase {
   double* prev[WS_FIELDS];  // fields at the previous feature call (physical step start)
   double* inc[WS_FIELDS];   // their increment over the last physical step
+  double* incp[WS_FIELDS];  // the increment over the step before (for the quadratic start)
 };
 
-// History (inc = fields - prev, prev = fields), the per-case, per-field RMS of inc into sc[c*8+f]
+// History (incp = inc, inc = fields - prev, prev = fields), the per-case, per-field RMS of inc into sc[c*8+f]
 // (1 where it is 0; ss is scratch of the same size; scale_out, if not null, receives sc as FP32)
 // and X[c][y][x][11] (FP32): fields, porous indicator, inc / sc.
 void launch_ws_features(const CaseDev* dc, const CaseCtl* dk, const WsCase* dw, int n, int H, int W, int has_prev,
@@ -30,9 +31,10 @@ void launch_ws_target(const CaseDev* dc, const CaseCtl* dk, const WsCase* dw, in
                       float* T, float* Wt, cudaStream_t s);
 // Candidates plain / extrapolated / learned (Y may be null: no learned candidate), initial
 // residuals into res[3c + k], choice[c] = k of the committed start (policy 0: smallest residual,
-// 1: the prediction, 2: plain).
+// 1: the prediction, 2: plain).  order 1: the extrapolated candidate is x + inc (linear);
+// order 2: x + (2 inc - incp) (quadratic through the last three step starts).
 void launch_ws_start(const CaseDev* dc, CaseCtl* dk, const WsCase* dw, int n, int H, int W, const double* sc,
-                     const float* Y, int ldy, const float* scale, int policy, unsigned long long* res, int* choice,
-                     cudaStream_t s);
+                     const float* Y, int ldy, const float* scale, int policy, int order, unsigned long long* res,
+                     int* choice, cudaStream_t s);
 
 }  // namespace acs

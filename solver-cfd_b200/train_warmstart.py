@@ -81,6 +81,8 @@ def main(argv=None):
     ap.add_argument("--load", default=None, help="skip generation and training; evaluate these weights")
     ap.add_argument("--eval-only", action="store_true",
                     help="no network: evaluate the plain and extrapolated starts only (--modes plain,extrap)")
+    ap.add_argument("--extrap-order", type=int, default=1, choices=[1, 2],
+                    help="evaluation: linear (1) or quadratic (2) extrapolated candidate")
     ap.add_argument("--autotune", action="store_true",
                     help="evaluate with the autotuner's launch shape for the held-out cases")
     a = ap.parse_args(argv)
@@ -150,7 +152,7 @@ def main(argv=None):
         log(f"launch shape {shape}")
     step_log = ws.StepLog(a.step_log) if a.step_log else None
     out = ws.evaluate(lambda: make_batch(pkg, held, launch_shape=shape), H, W, a.eval_steps, 1, net, norm,
-                      modes=modes, log=log, step_log=step_log)
+                      modes=modes, log=log, step_log=step_log, extrap_order=a.extrap_order)
     if step_log is not None:
         step_log.close()
     res = {}

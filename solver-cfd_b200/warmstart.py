@@ -28,7 +28,7 @@ import os
 
 import numpy as np
 
-from . import POLICY_BEST, START_PLAIN, WS_IN, WS_OUT, Batch
+from . import OPT_EXTRAP_ORDER, POLICY_BEST, START_PLAIN, WS_IN, WS_OUT, Batch
 from .unet import UNet, kernels as unet_kernels
 
 N_FIELDS = 5
@@ -139,7 +139,10 @@ class StepLog:
 class WarmStart:
     """Warm start of a Batch of cases drawn on one H x W canvas."""
 
-    def __init__(self, batch: Batch, H: int, W: int, net: UNet | None = None, norm: Normalizer | None = None):
+    def __init__(self, batch: Batch, H: int, W: int, net: UNet | None = None, norm: Normalizer | None = None,
+                 extrap_order: int = 1):
+        """extrap_order 2 makes the extrapolated candidate the quadratic through the last three
+        step starts (ACS_OPT_EXTRAP_ORDER)."""
         import torch
         self.torch = torch
         self.b = batch
@@ -151,6 +154,8 @@ class WarmStart:
         self.steps_done = 0
         batch.set_stream(torch.cuda.current_stream().cuda_stream)
         batch.ws_enable(H, W)
+        if extrap_order != 1:
+            batch.set_option(OPT_EXTRAP_ORDER, extrap_order)
         f32 = dict(dtype=torch.float32, device="cuda")
         self.X = torch.zeros(self.n * H * W * WS_IN, **f32)
         self.T = torch.zeros(self.n * H * W * WS_OUT, **f32)
@@ -323,7 +328,7 @@ def load(path, device="cuda"):
 
 
 def evaluate(make_batch, H, W, n_steps, itc0, net=None, norm=None, modes=("plain", "extrap", "learned"),
-             log=None, step_log: StepLog | None = None):
+             log=None, step_log: StepLog | None = None, extrap_order: int = 1):
     """Run fresh copies of the same cases for n_steps in each mode.  Returns per mode the
     iterations [n, n_steps], the seconds per step (device time, CUDA events around the whole
     step: features, network, start selection and the pseudo-time loop), the fraction of cases
@@ -333,7 +338,7 @@ def evaluate(make_batch, H, W, n_steps, itc0, net=None, norm=None, modes=("plain
     out = {}
     for mode in modes:
         b = make_batch()
-        ws = WarmStart(b, H, W, net if mode == "learned" else None, norm)
+        ws = WarmStart(b, H, W, net if mode == "learned" else None, norm, extrap_order=extrap_order)
         if step_log is not None:
             step_log.label = mode
             ws.log = step_log

@@ -2,7 +2,8 @@
 
 * a plain-policy start leaves the loop bit-identical to a run without the hooks;
 * the feature canvas holds the downloaded fields and increments at their staggered pixels;
-* the extrapolated start is fields + increment with the oracle's boundary passes, bit for bit;
+* the extrapolated start is fields + increment (or the quadratic through the last three step
+  starts) with the oracle's boundary passes, bit for bit;
 * the initial residuals are the oracle's stage-1 momentum and pressure residual maxima;
 * ablation: a network trained on snapshots of eight cases starts two held-out cases; the
   pseudo-iterations per step are compared with the plain start (the method without the
@@ -116,6 +117,67 @@ def test_features_and_extrapolated_start(gpu, orc, ws_mod):
     r_plain = _initial_residual(oc, prm, mesh, cur, cur["um_tau"], cur["vm_tau"], cur["pn"])
     assert abs(res0[0, 0] - r_plain) <= 1e-13 * r_plain, (res0[0, 0], r_plain)
     assert np.isnan(res0[0, 2])
+
+
+def _expected_start(oc, ut, vt, pp, Tt, Ct):
+    ut, vt, pp, Tt, Ct = (np.asfortranarray(a) for a in (ut, vt, pp, Tt, Ct))
+    oc.bc_uv(ut, vt)
+    oc.bc_p(pp)
+    oc.bc_z(Tt)
+    oc.bc_c(Ct)
+    return ut, vt, pp, Tt, Ct
+
+
+def _assert_start(got, exp):
+    ut, vt, pp, Tt, Ct = exp
+    assert np.array_equal(got["um_tau"], ut)
+    assert np.array_equal(mask_dead("vm", got["vm_tau"], 1), mask_dead("vm", vt, 1))
+    assert np.array_equal(got["p"], pp) and np.array_equal(got["pn"], pp)
+    assert np.array_equal(got["T_tau"], Tt) and np.array_equal(got["C_tau"], Ct)
+
+
+def test_quadratic_extrapolated_start(gpu, orc, ws_mod):
+    """ACS_OPT_EXTRAP_ORDER = 2: with two increments (three feature calls) the extrapolated
+    candidate is x2 + (2 (x2 - x1) - (x1 - x0)) with the oracle's boundary passes, bit for bit;
+    with one increment it is still the linear x1 + (x1 - x0)."""
+    pkg = gpu
+    prm, mesh, st, itc0 = _case(pkg)
+    oc = orc.OracleCase(prm, mesh)
+    keys = ("um", "vm", "pn", "T", "C")
+    # one increment: linear
+    b = _batch(pkg, [(prm, mesh, st)])
+    b.set_option(pkg.OPT_EXTRAP_ORDER, 2)
+    w = ws_mod.WarmStart(b, 32, 32)
+    x0 = b.get_state(0)
+    w.features()
+    itc, _, _, _ = b.run(1, np.ones(1, np.int32))
+    x1 = b.get_state(0)
+    w.features()
+    chosen, _ = b.set_start(None, 8, None, pkg.POLICY_PREDICTED)
+    assert chosen[0] == 1
+    _assert_start(b.get_state(0), _expected_start(oc, *(x1[k] + (x1[k] - x0[k]) for k in keys)))
+    b.close()
+    # two increments: quadratic
+    b = _batch(pkg, [(prm, mesh, st)])
+    b.set_option(pkg.OPT_EXTRAP_ORDER, 2)
+    with pytest.raises(pkg.AcsError):
+        b.set_option(pkg.OPT_EXTRAP_ORDER, 3)
+    w = ws_mod.WarmStart(b, 32, 32)
+    w.features()
+    itc, _, _, _ = b.run(1, np.ones(1, np.int32))
+    w.features()
+    itc, _, _, _ = b.run(1, itc)
+    x2 = b.get_state(0)
+    w.features()
+    chosen, res0 = b.set_start(None, 8, None, pkg.POLICY_PREDICTED)
+    assert chosen[0] == 1
+    exp = _expected_start(oc, *(x2[k] + (2.0 * (x2[k] - x1[k]) - (x1[k] - x0[k])) for k in keys))
+    _assert_start(b.get_state(0), exp)
+    r_ref = _initial_residual(oc, prm, mesh, x2, exp[0], exp[1], exp[2])
+    assert abs(res0[0, 1] - r_ref) <= 1e-13 * r_ref, (res0[0, 1], r_ref)
+    _, it, _, status = b.run(1, itc)
+    assert status[0] == pkg.CASE_DONE and it[0, 0] >= 1
+    b.close()
 
 
 def _initial_residual(oc, prm, mesh, cur, ut, vt, pn):
