@@ -14,6 +14,9 @@ from the same state and reported beside it (``plain_gpu``).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--arith exact|fast]
     python bench.py --impl reference ...   # the CPU implementation of the loop on host cores
 
+Warm-start policy options (off by default): --extrap-order 2 (quadratic extrapolated
+candidate), --warm-eps E (residual tolerance of the warm-started cases of each step).
+
 Multi-GPU (torchrun): each rank runs its own replica of the workload (cases are independent, so
 there is no exchange on the data path); the elapsed time is the max over ranks.
 """
