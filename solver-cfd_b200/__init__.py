@@ -52,7 +52,7 @@ POLICY_BEST, POLICY_PREDICTED, POLICY_PLAIN = 0, 1, 2
 START_PLAIN, START_EXTRAP, START_LEARNED = 0, 1, 2
 OPT_ENGINE, OPT_NODES_PER_CTA, OPT_L1_LOADS, OPT_THREADS, OPT_CTAS_PER_SM, OPT_STAGED = 1, 2, 3, 4, 5, 6
 OPT_EXTRAP_ORDER = 7
-ENGINE_CLUSTER, ENGINE_GRAPH = 0, 1
+ENGINE_CLUSTER, ENGINE_GRAPH, ENGINE_TILE = 0, 1, 2
 
 
 class AcsError(RuntimeError):

@@ -30,6 +30,7 @@ SOURCES = {
     "control.cu": ["-fmad=false"],
     "engine_fast.cu": [],
     "kernels_fast.cu": [],
+    "tile_engine.cu": [],
     "fast_tables.cu": [],
     "noalloc.cu": [],
     "warmstart.cu": ["-fmad=false"],
@@ -38,7 +39,7 @@ SOURCES = {
     "../unet/csrc/unet_ops.cu": [],
 }
 CXX_SOURCES = {"mesh.cpp": ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"]}
-HEADERS = [os.path.join(ROOT, "include", "unet.h"), "acs_dev.cuh", "kernels.h", "fast.h", "engine.cuh", "engine_api.h", "points_exact.cuh", "points_fast.cuh", "bc_exact.cuh", "warmstart.h",
+HEADERS = [os.path.join(ROOT, "include", "unet.h"), "acs_dev.cuh", "kernels.h", "fast.h", "engine.cuh", "engine_api.h", "points_exact.cuh", "points_fast.cuh", "bc_exact.cuh", "warmstart.h", "tile_engine.h",
            "../unet/csrc/gemm_tc.cuh"]
 
 

@@ -24,23 +24,42 @@ namespace acs {
 // per-row    table MY[j] = {y(j)-y(j-1), 1/(y(j)-y(j-1)), ym(j+1)-ym(j), 1/(ym(j+1)-ym(j))}
 struct Met { double d, rd, dm, rdm; };
 
-__device__ __forceinline__ Met mx(const CaseDev& d, int i) {
-  const double2 a = __ldg(reinterpret_cast<const double2*>(d.mx) + 2 * i);
-  const double2 b = __ldg(reinterpret_cast<const double2*>(d.mx) + 2 * i + 1);
+// Entry k of a metric table (4 doubles) from global memory through the read-only path.
+__device__ __forceinline__ Met met_ldg(const double* t, int k) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(t) + 2 * k);
+  const double2 b = __ldg(reinterpret_cast<const double2*>(t) + 2 * k + 1);
   return {a.x, a.y, b.x, b.y};
 }
-__device__ __forceinline__ Met my(const CaseDev& d, int j) {
-  const double2 a = __ldg(reinterpret_cast<const double2*>(d.my) + 2 * j);
-  const double2 b = __ldg(reinterpret_cast<const double2*>(d.my) + 2 * j + 1);
-  return {a.x, a.y, b.x, b.y};
-}
+__device__ __forceinline__ Met mx(const CaseDev& d, int i) { return met_ldg(d.mx, i); }
+__device__ __forceinline__ Met my(const CaseDev& d, int j) { return met_ldg(d.my, j); }
+
+// Load policies: ld() reads a field, met() an entry of a metric table.
 // Loads of arrays written by other CTAs of the cluster: from L2 (.cg) or through L1 (.ca); the
 // cluster barrier's release/acquire pair orders the writes before the reads in both cases.
-struct LdL2 { static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldcg(a + q); } };
-struct LdL1 { static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldca(a + q); } };
+struct LdL2 {
+  static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldcg(a + q); }
+  static __device__ __forceinline__ Met met(const double* t, int k) { return met_ldg(t, k); }
+};
+struct LdL1 {
+  static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldca(a + q); }
+  static __device__ __forceinline__ Met met(const double* t, int k) { return met_ldg(t, k); }
+};
 // Generic loads: the staged engine reads its stencil arrays from shared memory and the rest from
 // global memory written by this CTA or before the cluster barrier.
-struct LdGen { static __device__ __forceinline__ double ld(const double* a, long long q) { return a[q]; } };
+struct LdGen {
+  static __device__ __forceinline__ double ld(const double* a, long long q) { return a[q]; }
+  static __device__ __forceinline__ Met met(const double* t, int k) { return met_ldg(t, k); }
+};
+// Everything from shared memory: the tile engine stages the fields and slices of the metric
+// tables (CaseDev::mx/my then point into those slices) before it computes.
+struct LdShared {
+  static __device__ __forceinline__ double ld(const double* a, long long q) { return a[q]; }
+  static __device__ __forceinline__ Met met(const double* t, int k) {
+    const double2 a = reinterpret_cast<const double2*>(t)[2 * k];
+    const double2 b = reinterpret_cast<const double2*>(t)[2 * k + 1];
+    return {a.x, a.y, b.x, b.y};
+  }
+};
 
 // QUICK face value seen from the face's upstream side (equations.f90:27-70 rearranged):
 // flux > 0 takes 0.75 of the upwind node, 0.375 of the downwind node, -0.125 of the far upwind.
@@ -53,15 +72,21 @@ template <class L>
 struct PtFastT {
   static __device__ __forceinline__ double ld(const double* a, long long q) { return L::ld(a, q); }
   static __device__ __forceinline__ double F(const double* a, long long q) { return L::ld(a, q); }
+  static __device__ __forceinline__ Met MX(const CaseDev& d, int i) { return L::met(d.mx, i); }
+  static __device__ __forceinline__ Met MY(const CaseDev& d, int j) { return L::met(d.my, j); }
 
   // u-momentum residual RU at node (i,j)
   static __device__ __forceinline__ double ru(const CaseDev& d, const double* um, const double* vm,
                                               const double* p, int i, int j) {
-    const int P = d.pitch;
-    const long long q = lin(i, j, P);
-    const bool por = d.mask[q];
+    const long long q = lin(i, j, d.pitch);
+    return ru_at(d, um, vm, p, d.pitch, q, d.mask[q] != 0, i, j);
+  }
+  // Same, with the fields indexed by q and row stride P (a shared-memory tile, or the case array
+  // itself) and the node's porous flag given.
+  static __device__ __forceinline__ double ru_at(const CaseDev& d, const double* um, const double* vm,
+                                                 const double* p, int P, long long q, bool por, int i, int j) {
     const double e = por ? d.phi : 1.0, ie = por ? d.fc[FC_IPHI] : 1.0;
-    const Met X = mx(d, i), Y = my(d, j), Yn = my(d, j + 1);
+    const Met X = MX(d, i), Y = MY(d, j), Yn = MY(d, j + 1);
     const double uP = F(um, q), uW = F(um, q - 1), uE = F(um, q + 1), uS = F(um, q - P), uN = F(um, q + P);
     const double hx = 0.5 * X.d * ie, hy = 0.5 * Y.dm * ie;
     const double fn = (F(vm, q + P) + F(vm, q + P - 1)) * hx;
@@ -77,7 +102,7 @@ struct PtFastT {
     } else {
       conv = fw * upw_face(fw, uW, uP) - fe * upw_face(fe, uP, uE) + fs * upw_face(fs, uS, uP) - fn * upw_face(fn, uP, uN);
     }
-    const double Xw = mx(d, i - 1).rdm;  // 1/(xm(i)-xm(i-1))
+    const double Xw = MX(d, i - 1).rdm;  // 1/(xm(i)-xm(i-1))
     const double diff = e * d.fc[FC_IRE] *
                         (X.d * (Yn.rd * (uN - uP) - Y.rd * (uP - uS)) + Y.dm * (X.rdm * (uE - uP) - Xw * (uP - uW)));
     double r = X.rd * Y.rd * (conv + diff) - e * (F(p, q) - F(p, q - 1)) * X.rd;
@@ -96,11 +121,17 @@ struct PtFastT {
   // v-momentum residual RV at node (i,j)
   static __device__ __forceinline__ double rv(const CaseDev& d, const double* um, const double* vm,
                                               const double* p, const double* T, int i, int j) {
-    const int P = d.pitch;
-    const long long q = lin(i, j, P);
-    const bool por = d.mask[q];
+    const long long q = lin(i, j, d.pitch);
+    const double T0 = (d.flags & F_BUOY) ? F(T, q) : 1.0, T1 = (d.flags & F_BUOY) ? F(T, q - d.pitch) : 1.0;
+    return rv_at(d, um, vm, p, T0, T1, d.pitch, q, d.mask[q] != 0, i, j);
+  }
+  // Same, fields indexed by q with row stride P; T0 = T(i,j), T1 = T(i,j-1) (read only with
+  // buoyancy) and the node's porous flag given.
+  static __device__ __forceinline__ double rv_at(const CaseDev& d, const double* um, const double* vm,
+                                                 const double* p, double T0, double T1, int P, long long q,
+                                                 bool por, int i, int j) {
     const double e = por ? d.phi : 1.0, ie = por ? d.fc[FC_IPHI] : 1.0;
-    const Met X = mx(d, i), Xe = mx(d, i + 1), Y = my(d, j), Ys = my(d, j - 1);
+    const Met X = MX(d, i), Xe = MX(d, i + 1), Y = MY(d, j), Ys = MY(d, j - 1);
     const double vP = F(vm, q), vW = F(vm, q - 1), vE = F(vm, q + 1), vS = F(vm, q - P), vN = F(vm, q + P);
     const double hx = 0.5 * X.dm * ie, hy = 0.5 * Y.d * ie;
     const double fn = (vP + vN) * hx;
@@ -124,7 +155,7 @@ struct PtFastT {
       const double dydudx = X.dm * (F(um, q + 1) - F(um, q)) * X.rdm - X.dm * (F(um, q + 1 - P) - F(um, q - P)) * X.rdm;
       r += d.b_art * (dydudx + dvdydy);
     }
-    if (d.flags & F_BUOY) r += d.InvFr2 * (1.0 - 2.0 / (F(T, q) + F(T, q - P)));
+    if (d.flags & F_BUOY) r += d.InvFr2 * (1.0 - 2.0 / (T0 + T1));
     if (por) {
       const double uP = F(um, q);
       r -= e * vP * (d.fc[FC_IREDA] + d.fc[FC_CFS] * sqrt(fma(uP, uP, vP * vP)));
@@ -136,13 +167,19 @@ struct PtFastT {
   template <bool IS_C>
   static __device__ __forceinline__ double rs(const CaseDev& d, const double* un, const double* vn,
                                               const double* z, int i, int j) {
-    const int P = d.pitch;
-    const long long q = lin(i, j, P);
-    const bool por = d.mask[q];
-    const Met X = mx(d, i), Xe = mx(d, i + 1), Y = my(d, j), Yn = my(d, j + 1);
-    const double zp = F(z, q), ze = F(z, q + 1), zw = F(z, q - 1), zn = F(z, q + P), zs = F(z, q - P);
-    const double conv = 0.5 * (Y.dm * ((ze + zp) * F(un, q + 1) - (zw + zp) * F(un, q)) +
-                               X.dm * ((zn + zp) * F(vn, q + P) - (zs + zp) * F(vn, q)));
+    const long long q = lin(i, j, d.pitch);
+    return rs_at<IS_C>(d, un, vn, d.pitch, q, z, d.pitch, q, d.mask[q] != 0, i, j);
+  }
+  // Same, un/vn indexed by qu with row stride Pu, z by qz with row stride Pz, the node's porous
+  // flag given.
+  template <bool IS_C>
+  static __device__ __forceinline__ double rs_at(const CaseDev& d, const double* un, const double* vn, int Pu,
+                                                 long long qu, const double* z, int Pz, long long qz, bool por,
+                                                 int i, int j) {
+    const Met X = MX(d, i), Xe = MX(d, i + 1), Y = MY(d, j), Yn = MY(d, j + 1);
+    const double zp = F(z, qz), ze = F(z, qz + 1), zw = F(z, qz - 1), zn = F(z, qz + Pz), zs = F(z, qz - Pz);
+    const double conv = 0.5 * (Y.dm * ((ze + zp) * F(un, qu + 1) - (zw + zp) * F(un, qu)) +
+                               X.dm * ((zn + zp) * F(vn, qu + Pu) - (zs + zp) * F(vn, qu)));
     const double k = IS_C ? d.fc[FC_IRESC] : d.fc[FC_IPE];
     const double diff = k * (Y.dm * (Xe.rd * (ze - zp) - X.rd * (zp - zw)) + X.dm * (Yn.rd * (zn - zp) - Y.rd * (zp - zs)));
     const double icap = por ? d.fc[FC_IPHI] : 1.0;
@@ -153,17 +190,24 @@ struct PtFastT {
   // solve_P at one node: with RP frozen the three stages give pn = p + dtau*beta*RP
   static __device__ __forceinline__ double p_update(const CaseDev& d, const double* p, const double* un,
                                                     const double* vn, int i, int j, double* r) {
-    const int P = d.pitch;
-    const long long q = lin(i, j, P);
-    const Met X = mx(d, i), Y = my(d, j);
+    const long long q = lin(i, j, d.pitch);
+    return F(p, q) + p_incr_at(d, un, vn, d.pitch, q, i, j, r);
+  }
+  // dtau*beta*RP at (i,j) with un, vn indexed by q and row stride P (also returned in *r)
+  static __device__ __forceinline__ double p_incr_at(const CaseDev& d, const double* un, const double* vn, int P,
+                                                     long long q, int i, int j, double* r) {
+    const Met X = MX(d, i), Y = MY(d, j);
     double RP = -((F(un, q + 1) - F(un, q)) * Y.dm + (F(vn, q + P) - F(vn, q)) * X.dm);
     if (d.continuity == 1) RP *= X.rdm * Y.rdm;
     *r = d.fc[FC_DTB] * RP;
-    return F(p, q) + *r;
+    return *r;
   }
 };
 
 // Read-only loads: in a per-stage kernel no array it reads is written during the launch.
-struct LdRO { static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldg(a + q); } };
+struct LdRO {
+  static __device__ __forceinline__ double ld(const double* a, long long q) { return __ldg(a + q); }
+  static __device__ __forceinline__ Met met(const double* t, int k) { return met_ldg(t, k); }
+};
 
 }  // namespace acs

@@ -22,6 +22,7 @@
 #include "fast.h"
 #include "engine_api.h"
 #include "kernels.h"
+#include "tile_engine.h"
 #include "warmstart.h"
 
 namespace acs {
@@ -98,7 +99,13 @@ struct Batch {
   long long launches = 0;
   long long body_kernels = 0;
   int graph_steps = -1;  // n_steps the graph's loop bound was built for
-  int engine = 0;        // 0 = persistent cluster engine, 1 = graph of per-stage kernels
+  int engine = 0;        // 0 = persistent cluster engine, 1 = graph of per-stage kernels,
+                         // 2 = graph of TMA-tiled kernels (tile_engine.cu)
+  // tile engine: tile table, tensor maps, TMA timeout word (set up on first use)
+  Tile* d_tetiles = nullptr;
+  int n_tetiles = 0;
+  TeMaps* d_temaps = nullptr;
+  int* d_te_err = nullptr;
   int nodes_per_cta = 1536;
   int l1_loads = 1;      // FAST engine: load cluster-written arrays through L1
   int threads = 512;     // FAST engine: threads per CTA (256 or 512)
@@ -136,6 +143,9 @@ struct Batch {
     if (d_err) cudaFree(d_err);
     if (h_flag) cudaFreeHost(h_flag);
     if (d_cases) cudaFree(d_cases);
+    if (d_tetiles) cudaFree(d_tetiles);
+    if (d_temaps) cudaFree(d_temaps);
+    if (d_te_err) cudaFree(d_te_err);
     for (auto s : side) cudaStreamDestroy(s);
     for (auto e : ev) cudaEventDestroy(e);
     if (own_stream && stream) cudaStreamDestroy(stream);
@@ -167,13 +177,9 @@ struct Batch {
   }
 };
 
-namespace {
-
-int validate(const acs_grid& g, const acs_params& p) {
-  if (!g.x || !g.y || !g.xm || !g.ym || !g.epsilon1 || !g.liga_poros) return fail(ACS_E_ARG, "null grid array");
-  if (g.imax != p.imax || g.jmax != p.jmax) return fail(ACS_E_ARG, "grid and params disagree on imax/jmax");
-  if (p.imax < kMinN || p.jmax < kMinN || p.imax > kMaxN || p.jmax > kMaxN)
-    return fail(ACS_E_SIZE, "imax and jmax must lie in [6, 32768]");
+// Checks of the parameter block that every entry point taking an acs_params shares (sizes are
+// checked by the caller, whose limits differ).
+int validate_params(const acs_params& p) {
   if (p.scheme != 0 && p.scheme != 1) return fail(ACS_E_ARG, "scheme must be 0 or 1");
   if (p.bc != 0 && p.bc != 1) return fail(ACS_E_ARG, "bc must be 0 or 1");
   if (p.arith != ACS_ARITH_EXACT && p.arith != ACS_ARITH_FAST) return fail(ACS_E_ARG, "arith must be 0 or 1");
@@ -181,6 +187,16 @@ int validate(const acs_grid& g, const acs_params& p) {
   if (p.continuity != 0 && p.continuity != 1) return fail(ACS_E_ARG, "continuity must be 0 or 1");
   if (!(p.Re > 0) || !(p.Pe > 0) || !(p.Sc > 0) || !(p.Da > 0)) return fail(ACS_E_ARG, "Re, Pe, Sc, Da must be positive");
   return ACS_OK;
+}
+
+namespace {
+
+int validate(const acs_grid& g, const acs_params& p) {
+  if (!g.x || !g.y || !g.xm || !g.ym || !g.epsilon1 || !g.liga_poros) return fail(ACS_E_ARG, "null grid array");
+  if (g.imax != p.imax || g.jmax != p.jmax) return fail(ACS_E_ARG, "grid and params disagree on imax/jmax");
+  if (p.imax < kMinN || p.jmax < kMinN || p.imax > kMaxN || p.jmax > kMaxN)
+    return fail(ACS_E_SIZE, "imax and jmax must lie in [6, 32768]");
+  return validate_params(p);
 }
 
 // Binary porous structure (eps, liga) in {(1,0), (phi,1)} for one phi.
@@ -507,6 +523,8 @@ void launch_timed_kernel(Batch& b, int kernel) {
     case 2: (b.use_fast ? launch_p_fast : launch_p_exact)(b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
     case 3: (b.use_fast ? launch_s_stage_fast : launch_s_stage_exact)(false, 1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
     case 4: (b.use_fast ? launch_s_stage_fast : launch_s_stage_exact)(true, 1, b.dc, b.dk, b.dtiles, b.ntiles, b.stream); break;
+    case 5: te_launch_uv(2, b.dc, b.dk, b.d_tetiles, b.n_tetiles, b.d_temaps, b.d_te_err, b.stream); break;
+    case 6: te_launch_ptc(b.dc, b.dk, b.d_tetiles, b.n_tetiles, b.d_temaps, b.d_te_err, b.stream); break;
   }
 }
 
@@ -514,6 +532,35 @@ bool any_scalars(const Batch& b) {
   for (auto& p : b.prm)
     if (p.solve_scalars) return true;
   return false;
+}
+
+// Tile engine set-up: tile table over every case, a tensor map per case buffer and box size.
+int te_setup(Batch& b) {
+  if (b.d_temaps) return ACS_OK;
+  if (!b.use_fast) return fail(ACS_E_UNSUPPORTED, "the tile engine computes in the FAST arithmetic only");
+  std::vector<Tile> tiles;
+  for (int c = 0; c < b.n; ++c) te_case_tiles(c, b.hc[c].pitch, b.hc[c].ny, tiles);
+  std::vector<TeMaps> maps(b.n);
+  const int er = te_encode_maps(b.hc, maps.data());
+  if (er) return fail(ACS_E_CUDA, er == 1 ? "cuTensorMapEncodeTiled is not available from the driver"
+                                           : "cuTensorMapEncodeTiled rejected a case buffer");
+  CU(te_prepare());
+  CU(cudaMalloc(&b.d_tetiles, sizeof(Tile) * tiles.size()));
+  CU(cudaMalloc(&b.d_temaps, sizeof(TeMaps) * b.n));
+  CU(cudaMalloc(&b.d_te_err, sizeof(int)));
+  CU(cudaMemcpy(b.d_tetiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(b.d_temaps, maps.data(), sizeof(TeMaps) * b.n, cudaMemcpyHostToDevice));
+  CU(cudaMemset(b.d_te_err, 0, sizeof(int)));
+  b.n_tetiles = (int)tiles.size();
+  return ACS_OK;
+}
+
+// one pseudo-iteration of the tile engine: U/V stages 1-3, P + T/C, control
+void te_iteration(Batch& b) {
+  for (int s = 1; s <= 3; ++s) te_launch_uv(s, b.dc, b.dk, b.d_tetiles, b.n_tetiles, b.d_temaps, b.d_te_err, b.stream);
+  te_launch_ptc(b.dc, b.dk, b.d_tetiles, b.n_tetiles, b.d_temaps, b.d_te_err, b.stream);
+  k_control<<<b.n, 256, 0, b.stream>>>(b.dc, b.dk, b.d_iters, b.d_err, b.d_nactive);
+  b.launches += 5;
 }
 
 // one pseudo-iteration (main.f90:122-150) for every active case
@@ -556,7 +603,8 @@ int build_graph(Batch& b, int n_steps) {
       e = cudaStreamBeginCaptureToGraph(b.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
       if (e == cudaSuccess) {
         const long long l0 = b.launches;
-        seq_iteration(b);
+        if (b.engine == 2) te_iteration(b);
+        else seq_iteration(b);
         k_loop_cond<<<1, 1, 0, b.stream>>>(b.d_nactive, b.d_iter, max_total_iterations(b, n_steps), h);
         b.body_kernels = b.launches - l0 + 1;
         e = cudaStreamEndCapture(b.stream, &body);
@@ -579,7 +627,8 @@ int build_graph(Batch& b, int n_steps) {
   cudaGraph_t g;
   CU(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
   const long long l0 = b.launches;
-  seq_iteration(b);
+  if (b.engine == 2) te_iteration(b);
+  else seq_iteration(b);
   k_loop_flag<<<1, 1, 0, b.stream>>>(b.d_nactive, b.d_iter, d_flag);
   b.body_kernels = b.launches - l0 + 1;
   CU(cudaStreamEndCapture(b.stream, &g));
@@ -652,11 +701,29 @@ int run_batch(Batch& b, int n_steps, int* itc, int* iters, double* err, int* sta
 
 int run_graph(Batch& b, int n_steps) {
   int r;
+  if (b.engine == 2) {
+    r = te_setup(b);
+    if (r) return r;
+  }
   // the graph bakes in the loop bound; rebuild when n_steps changes the bound
   if (!b.gexec || b.graph_steps != n_steps) {
     r = build_graph(b, n_steps);
     if (r) return r;
     b.graph_steps = n_steps;
+  }
+  long long pre = 0;
+  if (b.engine == 2) {
+    // After an upload (or a committed warm start) um_tau / vm_tau may not satisfy the boundary
+    // passes, and the reference's first solve_U / solve_V read them before their bcUV side
+    // effects: that iteration runs with the per-stage kernels in the reference's order.
+    bool dirty = false;
+    for (int c = 0; c < b.n; ++c) dirty |= b.hk[c].tau_dirty != 0;
+    if (dirty) {
+      const long long l0 = b.launches;
+      seq_iteration(b);
+      pre = b.launches - l0;
+      CU(cudaMemsetAsync(b.d_nactive, 0, sizeof(int), b.stream));
+    }
   }
   if (b.graph_conditional) {
     CU(cudaGraphLaunch(b.gexec, b.stream));
@@ -674,7 +741,12 @@ int run_graph(Batch& b, int n_steps) {
   }
   long long iters_done = 0;
   CU(cudaMemcpy(&iters_done, b.d_iter, sizeof(long long), cudaMemcpyDeviceToHost));
-  b.launches = iters_done * b.body_kernels;
+  b.launches = iters_done * b.body_kernels + pre;
+  if (b.engine == 2) {
+    int te_err = 0;
+    CU(cudaMemcpy(&te_err, b.d_te_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (te_err) return fail(ACS_E_CUDA, "tile engine: a TMA wait timed out (the results of this run are not valid)");
+  }
   return ACS_OK;
 }
 
@@ -932,8 +1004,12 @@ int acs_batch_set_start(acs_batch* h, const float* Y, int ldy, const float* scal
 }
 
 int acs_batch_time_kernel(acs_batch* h, int kernel, int reps, double* ms_mean, long long* cells) {
-  if (!h || !ms_mean || reps <= 0 || kernel < 0 || kernel > 4) return acs::fail(ACS_E_ARG, "bad argument");
+  if (!h || !ms_mean || reps <= 0 || kernel < 0 || kernel > 6) return acs::fail(ACS_E_ARG, "bad argument");
   Batch& b = *h->b;
+  if (kernel >= 5) {
+    int r = acs::te_setup(b);
+    if (r) return r;
+  }
   std::vector<acs::CaseCtl> saved = b.hk;
   long long nc = 0;
   for (int c = 0; c < b.n; ++c) {
@@ -941,7 +1017,7 @@ int acs_batch_time_kernel(acs_batch* h, int kernel, int reps, double* ms_mean, l
     b.hk[c].scalars = 1;
     const int nx = b.hc[c].nx, ny = b.hc[c].ny;
     nc += kernel == 0 ? (long long)(nx - 3) * (ny - 2) : kernel == 1 ? (long long)(nx - 2) * (ny - 3)
-                                                                     : (long long)(nx - 2) * (ny - 2);
+          : kernel >= 5 ? (long long)nx * ny : (long long)(nx - 2) * (ny - 2);
   }
   int r = acs::push_ctl(b);
   if (r) return r;
@@ -949,9 +1025,26 @@ int acs_batch_time_kernel(acs_batch* h, int kernel, int reps, double* ms_mean, l
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
   auto one = [&]() { acs::launch_timed_kernel(b, kernel); };
-  if (kernel == 2)  // the pressure kernel writes pn: keep a copy in stage scratch
-    for (int c = 0; c < b.n; ++c)
-      CU(cudaMemcpyAsync(b.hc[c].S[1], b.hc[c].P[b.hk[c].rp[1]], 8 * b.hc[c].n_elems, cudaMemcpyDeviceToDevice, b.stream));
+  // the pressure kernels write pn (and the tile engine's P/T/C kernel T and C of role n_tau): keep
+  // copies in stage scratch
+  auto save = [&](bool back) -> int {
+    for (int c = 0; c < b.n; ++c) {
+      const acs::CaseDev& d = b.hc[c];
+      const acs::CaseCtl& k = b.hk[c];
+      double* live[3] = {d.P[k.rp[1]], d.T[k.rt[acs::R_NTAU]], d.C[k.rc[acs::R_NTAU]]};
+      const int nf = kernel == 6 ? 3 : 1;
+      for (int f = 0; f < nf; ++f) {
+        double* a = back ? live[f] : d.S[1 + f];
+        double* z = back ? d.S[1 + f] : live[f];
+        CU(cudaMemcpyAsync(a, z, 8 * d.n_elems, cudaMemcpyDeviceToDevice, b.stream));
+      }
+    }
+    return ACS_OK;
+  };
+  if (kernel == 2 || kernel == 6) {
+    r = save(false);
+    if (r) return r;
+  }
   one();  // warm
   CU(cudaEventRecord(e0, b.stream));
   for (int i = 0; i < reps; ++i) one();
@@ -962,9 +1055,10 @@ int acs_batch_time_kernel(acs_batch* h, int kernel, int reps, double* ms_mean, l
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   CU(cudaGetLastError());
-  if (kernel == 2)
-    for (int c = 0; c < b.n; ++c)
-      CU(cudaMemcpyAsync(b.hc[c].P[b.hk[c].rp[1]], b.hc[c].S[1], 8 * b.hc[c].n_elems, cudaMemcpyDeviceToDevice, b.stream));
+  if (kernel == 2 || kernel == 6) {
+    r = save(true);
+    if (r) return r;
+  }
   *ms_mean = ms / reps;
   if (cells) *cells = nc;
   for (int c = 0; c < b.n; ++c) {  // the residual slots were touched; restore the control words
@@ -1003,10 +1097,20 @@ int acs_batch_set_option(acs_batch* h, int option, long long value) {
   if (!h) return acs::fail(ACS_E_ARG, "null handle");
   Batch& b = *h->b;
   switch (option) {
-    case ACS_OPT_ENGINE:
-      if (value != 0 && value != 1) return acs::fail(ACS_E_ARG, "engine must be 0 or 1");
+    case ACS_OPT_ENGINE: {
+      if (value < 0 || value > 2) return acs::fail(ACS_E_ARG, "engine must be 0, 1 or 2");
+      if (value == 2) {
+        int r = acs::te_setup(b);
+        if (r) return r;
+      }
+      if (b.engine != (int)value) {  // the captured loop body belongs to the previous engine
+        if (b.gexec) { cudaGraphExecDestroy(b.gexec); b.gexec = nullptr; }
+        if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
+        b.graph_steps = -1;
+      }
       b.engine = (int)value;
       return ACS_OK;
+    }
     case ACS_OPT_NODES_PER_CTA:
       if (value < 64 || value > (1 << 22)) return acs::fail(ACS_E_ARG, "nodes per CTA out of range");
       b.nodes_per_cta = (int)value;
