@@ -182,10 +182,14 @@ int acs_batch_time_kernel(acs_batch* b, int kernel, int reps, double* ms_mean, l
  * the grid's x, y, xm, ym as in acs_grid) and no handle.  Its scratch is one static device array
  * of ACS_STATIC_SCRATCH_BYTES that every GPU loading this library holds until exit; sizes beyond
  * ACS_STATIC_MAX_DIM per direction or round_up(imax+1,4)*(jmax+1) > ACS_STATIC_MAX_NODES are
- * rejected with ACS_E_SIZE.  The scratch address is looked up on the first call made on each
- * device, so make that first call before any stream capture.  All calls share the scratch: calls
- * that overlap on the GPU race.  The call synchronises `cuda_stream` (NULL = legacy default
- * stream) and writes *residual_u on the host.  Arithmetic as ACS_ARITH_EXACT. */
+ * rejected with ACS_E_SIZE.  The parameter block is checked as acs_create checks it (ACS_E_ARG
+ * for Re, Pe, Sc or Da <= 0, itc_max < 2, an unknown scheme, bc or continuity), and arith must be
+ * ACS_ARITH_EXACT, the arithmetic it computes in.  The scratch address is looked up on the first
+ * call made on each device, so make that first call before any stream capture; the address is
+ * kept for the life of the process and does not survive cudaDeviceReset (do not call this entry
+ * point again after a reset).  All calls share the scratch, which each call clears before use:
+ * calls that overlap on the GPU race.  The call synchronises `cuda_stream` (NULL = legacy default
+ * stream) and writes *residual_u on the host. */
 #define ACS_STATIC_MAX_DIM 4096
 #define ACS_STATIC_MAX_NODES 65536
 #define ACS_STATIC_SCRATCH_BYTES (5 * 1024 * 1024)

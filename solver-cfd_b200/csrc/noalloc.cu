@@ -12,9 +12,11 @@
 // the process exits.  Host code may not use the array's name as a device address: on the host the
 // symbol is a stand-in, so the device address is fetched once per device with
 // cudaGetSymbolAddress (on the first call made on that device; make that first call before any
-// stream capture) and passed to the kernels.  Every call overwrites the whole array, so calls
-// that overlap on the GPU (two streams, two host threads) race and must be serialised by the
-// caller.
+// stream capture) and passed to the kernels.  That cached address belongs to the context it was
+// taken in: after cudaDeviceReset the library's module is loaded again, so a caller that resets
+// the device must not call this entry point again in the same process.  Every call rewrites the
+// part of the array it uses (clearing it first), so calls that overlap on the GPU (two streams,
+// two host threads) race and must be serialised by the caller.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -27,6 +29,7 @@
 
 namespace acs {
 int fail(int code, const std::string& msg);
+int validate_params(const acs_params& p);  // solver.cu: the checks acs_create makes
 
 namespace {
 
@@ -40,7 +43,9 @@ constexpr size_t kMetricBytes = sizeof(double) * 4 * (kMaxDim + 3);
 constexpr size_t kFieldBytes = sizeof(double) * kMaxNodes;
 constexpr size_t kScratchBytes = kHead + kTileBytes + kMetricBytes + kFields * kFieldBytes;
 static_assert(kScratchBytes <= ACS_STATIC_SCRATCH_BYTES, "scratch layout exceeds the stated size");
-static_assert(sizeof(CaseDev) + sizeof(CaseCtl) + 256 <= kHead, "descriptor region too small");
+constexpr size_t kCtlOffset = 2048;                    // CaseDev at 0, CaseCtl at kCtlOffset
+static_assert(sizeof(CaseDev) <= kCtlOffset, "case descriptor overlaps the control word");
+static_assert(kCtlOffset + sizeof(CaseCtl) <= kHead, "control word overlaps the tile table");
 
 __device__ __align__(256) unsigned char g_scratch[ACS_STATIC_SCRATCH_BYTES];
 
@@ -65,6 +70,12 @@ int scratch_address(char** out) {
   return ACS_OK;
 }
 
+// Sets n doubles at p to v (the porosity padding; cudaMemset cannot write 1.0).
+__global__ void k_fill(double* p, long long n, double v) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    p[q] = v;
+}
+
 }  // namespace
 }  // namespace acs
 
@@ -83,16 +94,18 @@ extern "C" int acs_solve_u_static(const acs_params* p, const acs_grid* g, const 
     return fail(ACS_E_SIZE, "acs_solve_u_static: case too large for the static scratch (need imax, jmax <= " +
                                 std::to_string(kMaxDim) + " and round_up(imax+1, 4)*(jmax+1) <= " +
                                 std::to_string(kMaxNodes) + ")");
-  if (p->scheme != 0 && p->scheme != 1) return fail(ACS_E_ARG, "scheme must be 0 or 1");
-  if (p->bc != 0 && p->bc != 1) return fail(ACS_E_ARG, "bc must be 0 or 1");
+  int r = validate_params(*p);
+  if (r) return r;
+  if (p->arith != ACS_ARITH_EXACT)
+    return fail(ACS_E_ARG, "acs_solve_u_static computes in the EXACT arithmetic only (arith must be 0)");
   char* base = nullptr;
-  int r = scratch_address(&base);
+  r = scratch_address(&base);
   if (r) return r;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 
   // carve the scratch
   CaseDev* dcase = reinterpret_cast<CaseDev*>(base);
-  CaseCtl* dctl = reinterpret_cast<CaseCtl*>(base + 2048);
+  CaseCtl* dctl = reinterpret_cast<CaseCtl*>(base + kCtlOffset);
   Tile* dtiles = reinterpret_cast<Tile*>(base + kHead);
   double* metric = reinterpret_cast<double*>(base + kHead + kTileBytes);
   double* fld[kFields];
@@ -145,6 +158,14 @@ extern "C" int acs_solve_u_static(const acs_params* p, const acs_grid* g, const 
   CUS(cudaMemcpyAsync(const_cast<double*>(d.y) + 1, g->y, sizeof(double) * ny, D2D, s));
   CUS(cudaMemcpyAsync(const_cast<double*>(d.xm) + 1, g->xm, sizeof(double) * (nx + 1), D2D, s));
   CUS(cudaMemcpyAsync(const_cast<double*>(d.ym) + 1, g->ym, sizeof(double) * (ny + 1), D2D, s));
+  // The scratch keeps the previous call's contents.  Clear every field region this call uses
+  // (pitch padding, the row past jmax and the tail past the case included) so nothing of an
+  // earlier, larger call survives, and give the porosity padding the values of a fluid node
+  // (epsilon1 = 1, liga = 0).  None of this allocates.
+  const long long ne = (long long)pitch * (ny + 1);
+  for (int f = 1; f < kFields; ++f) CUS(cudaMemsetAsync(fld[f], 0, sizeof(double) * ne, s));
+  k_fill<<<64, 256, 0, s>>>(eps, ne, 1.0);
+  CUS(cudaGetLastError());
   // Fortran-layout inputs -> pitched scratch (leading dimension nx+1 for u, nx for v and cells)
   auto in2d = [&](double* dst, const double* src, int w, int h) {
     return cudaMemcpy2DAsync(dst, (size_t)pitch * 8, src, (size_t)w * 8, (size_t)w * 8, h, D2D, s);

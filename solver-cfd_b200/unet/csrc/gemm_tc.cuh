@@ -14,8 +14,9 @@
 // commit of the MMAs that read it has arrived.  The epilogue reads the accumulator with tcgen05.ld (32 lanes x 32 bit,
 // 16 columns per load): warp w owns TMEM lanes 32w..32w+31, i.e. tile rows 32w..32w+31.
 //
-// Every wait on an mbarrier is bounded; on a timeout the kernel records the failure in *err,
-// frees its tensor memory and returns.
+// Every wait on an mbarrier is bounded; on a timeout the kernel waits (bounded again) for the
+// commit of the last MMAs it issued, records the failure in *err, frees its tensor memory and
+// returns.  After *err is set the output is not valid and the caller should stop using the GEMM.
 #pragma once
 #include <cuda_bf16.h>
 #include <cstdint>
@@ -176,6 +177,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(GemmArgs a) {
   constexpr uint32_t idesc = umma_idesc(TC_BM, BN);
   bool ok = true;
   uint32_t phase = 0u;  // bit q: parity of the next completion of stage q's mbarrier
+  int last_commit = -1;  // the last slab whose MMAs thread 0 committed (same value in every thread)
 
   // slab t of this split goes to stage t % S; cp.async group g holds slab g
   auto load_tile = [&](int t) {
@@ -211,6 +213,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(GemmArgs a) {
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                    ::"r"(smem_u32(&bars[st])) : "memory");
     }
+    last_commit = i;
     // refill: slab i+S-1 goes to the stage the MMAs of slab i-1 read
     const int j = i + S - 1;
     if (j < nk) {
@@ -230,6 +233,15 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(GemmArgs a) {
     const int sp = t % S;
     ok = cta_wait(smem_u32(&bars[sp]), (phase >> sp) & 1u, wait_flag);
     phase ^= 1u << sp;
+  }
+  if (!ok && last_commit >= 0) {
+    // A wait timed out while MMAs may still run.  A tcgen05.commit arrives once every MMA this
+    // thread issued before it has completed, so one more bounded wait on the last commit (slab L
+    // is the (L / S)-th use of stage L % S) drains them all before the tensor memory is freed.
+    // If this wait times out too, nothing more can be done here: the error word tells the caller
+    // that the output, and the state of this context, are no longer reliable.
+    const int L = last_commit;
+    cta_wait(smem_u32(&bars[L % S]), (uint32_t)((L / S) & 1), wait_flag);
   }
   asm volatile("tcgen05.fence::after_thread_sync;");
   if (!ok) {

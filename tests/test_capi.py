@@ -46,3 +46,22 @@ def test_version_and_errors_without_device(pkg):
     assert L.acs_create(None, None, None) != 0
     assert L.acs_batch_create(None, None, 0, None) != 0
     assert pkg.reference_jmax(51) == 84
+
+
+def test_static_solve_u_checks_parameters_like_acs_create(pkg):
+    """The allocation-free solve_U rejects what acs_create rejects (here: a Darcy number of 0,
+    which would put sqrt(eps*Da) = 0 under a division) and the FAST arithmetic it does not
+    compute in, before it touches the device (the pointers are never dereferenced)."""
+    L = pkg.lib()
+    prm, mesh, _, _ = pkg.configs.channel_case(20, 16)
+    g = pkg.AcsGrid()
+    g.imax, g.jmax = prm.imax, prm.jmax
+    dummy = (ctypes.c_double * 1)()
+    g.x = g.y = g.xm = g.ym = g.epsilon1 = g.liga_poros = ctypes.cast(dummy, ctypes.POINTER(ctypes.c_double))
+    r = ctypes.c_double()
+    from dataclasses import replace
+    for bad in (replace(prm, Da=0.0), replace(prm, Re=-1.0), replace(prm, itc_max=1),
+                replace(prm, continuity=3), replace(prm, arith=pkg.ARITH_FAST)):
+        p = bad.struct()
+        code = L.acs_solve_u_static(ctypes.byref(p), ctypes.byref(g), 1, 1, 1, 1, 1, ctypes.byref(r), None)
+        assert code == pkg.ACS_E_ARG, (bad, code)

@@ -35,12 +35,9 @@ def _cases(pkg):
     yield "channel", prm, mesh
 
 
-@pytest.mark.parametrize("which", [0, 1])
-def test_static_solve_u_matches_handle(gpu, which):
-    import torch
-    pkg = gpu
+def _compare_calls(pkg, torch, name, prm, mesh, rng, calls):
+    """`calls` calls of the allocation-free solve_U, each compared with acs_solve_u."""
     L = pkg.lib()
-    name, prm, mesh = list(_cases(pkg))[which]
     nx, ny = prm.imax, prm.jmax
     handle = pkg.Case(prm, mesh)
     # grid on the device, in the acs_grid layout
@@ -50,8 +47,7 @@ def test_static_solve_u_matches_handle(gpu, which):
     ptrs = [C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_double)) for t in keep]
     g.x, g.y, g.xm, g.ym, g.epsilon1, g.liga_poros = ptrs
     p = prm.struct()
-    rng = np.random.default_rng(100 + which)
-    for call in range(2):  # two calls in a row share the static scratch
+    for call in range(calls):
         um = np.asfortranarray(rng.uniform(-1, 1, (nx + 1, ny)))
         um_tau = np.asfortranarray(rng.uniform(-1, 1, (nx + 1, ny)))
         vm_tau = np.asfortranarray(rng.uniform(-1, 1, (nx, ny + 1)))
@@ -73,6 +69,26 @@ def test_static_solve_u_matches_handle(gpu, which):
         vt_s = _host(d_vt, (nx, ny + 1))
         assert np.array_equal(un_s, un_h), (name, call)
         assert np.array_equal(mask_dead("vm_tau", vt_s, prm.bc), mask_dead("vm_tau", vt_h, prm.bc)), (name, call)
+    handle.close()
+
+
+@pytest.mark.parametrize("which", [0, 1])
+def test_static_solve_u_matches_handle(gpu, which):
+    import torch
+    name, prm, mesh = list(_cases(gpu))[which]
+    # two calls in a row share the static scratch
+    _compare_calls(gpu, torch, name, prm, mesh, np.random.default_rng(100 + which), 2)
+
+
+def test_static_solve_u_large_then_small(gpu):
+    """A smaller case right after a larger one: nothing the larger call left in the shared
+    scratch (padding, rows past jmax) may reach the smaller call's result."""
+    import torch
+    cases = list(_cases(gpu))
+    big, small = sorted(cases, key=lambda c: -(c[1].imax + 1) * (c[1].jmax + 1))
+    rng = np.random.default_rng(7)
+    _compare_calls(gpu, torch, *big, rng, 1)
+    _compare_calls(gpu, torch, *small, rng, 1)
 
 
 def test_static_solve_u_rejects_oversize(gpu):
