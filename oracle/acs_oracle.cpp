@@ -716,6 +716,12 @@ double orc_noise(uint64_t seed, uint64_t case_id, uint64_t field, uint64_t index
   return amp * (2.0 * u - 1.0);
 }
 
+// orc_noise at n indices (the case builders' initial perturbation, without a Python loop)
+void orc_noise_array(uint64_t seed, uint64_t case_id, uint64_t field, const uint64_t* index, long long n,
+                     double amp, double* out) {
+  for (long long k = 0; k < n; ++k) out[k] = orc_noise(seed, case_id, field, index[k], amp);
+}
+
 struct orc_case;
 orc_case* orc_create(const orc_params* prm, const double* x, const double* y, const double* xm,
                      const double* ym, const double* eps, const double* liga) {

@@ -69,6 +69,7 @@ def _declare(L):
     L.orc_mesh_channel.restype = C.c_int
     L.orc_noise.argtypes = [C.c_uint64] * 4 + [C.c_double]
     L.orc_noise.restype = C.c_double
+    L.orc_noise_array.argtypes = [C.c_uint64] * 3 + [C.POINTER(C.c_uint64), C.c_longlong, C.c_double, _D]
     L.orc_create.argtypes = [C.POINTER(OrcParams), _D, _D, _D, _D, _D, _D]
     L.orc_create.restype = C.c_void_p
     L.orc_destroy.argtypes = [C.c_void_p]
@@ -141,6 +142,13 @@ def _alloc_mesh(nx, ny):
 
 def noise(seed, case_id, field, index, amp):
     return lib().orc_noise(seed, case_id, field, index, amp)
+
+
+def noise_array(seed, case_id, field, index: np.ndarray, amp) -> np.ndarray:
+    idx = np.ascontiguousarray(index, dtype=np.uint64)
+    out = np.zeros(idx.size)
+    lib().orc_noise_array(seed, case_id, field, idx.ctypes.data_as(C.POINTER(C.c_uint64)), idx.size, amp, _p(out))
+    return out
 
 
 STATE_FIELDS = ("um", "vm", "um_tau", "vm_tau", "um_n_tau", "vm_n_tau", "p", "pn",

@@ -23,6 +23,31 @@ import numpy as np
 from . import (ARITH_EXACT, BC_CHANNEL, SCHEME_QUICK, SCHEME_UPWIND, Params, field_shape,
                mesh_channel, mesh_reference, noise, noise_array, reference_jmax)
 
+# The case builders draw meshes and noise from a generator backend: by default this package's C
+# ABI (acs_mesh_channel, acs_noise, acs_noise_array); any module with the same mesh_channel(nx, ny,
+# Lx, Ly, stretch, block, porosity, block2), noise(seed, case_id, field, index, amp) and
+# noise_array(seed, case_id, field, index, amp) functions can stand in (the CPU oracle has all
+# three, so a run that must not load this package's library can still build the identical cases).
+_backend = None
+
+
+def use_backend(module) -> None:
+    """Make the case builders draw meshes and noise from `module` (None: this package)."""
+    global _backend
+    _backend = module
+
+
+def _mesh_channel(*a, **k):
+    return (_backend.mesh_channel if _backend is not None else mesh_channel)(*a, **k)
+
+
+def _noise_array(*a, **k):
+    return (_backend.noise_array if _backend is not None else noise_array)(*a, **k)
+
+
+def _noise(*a, **k):
+    return (_backend.noise if _backend is not None else noise)(*a, **k)
+
 # field ids of the noise generator (shared by specification with the oracle tests)
 NOISE_U, NOISE_V, NOISE_PARAM = 1, 2, 100
 
@@ -84,7 +109,7 @@ def channel_case(nx, ny, *, seed=0, case_id=0, Re=100.0, scheme=SCHEME_QUICK, bl
                  continuity=1):
     """Channel configuration.  Returns (params, mesh, state, itc0).  dtau=None picks
     stable_dtau() for the mesh."""
-    mesh = mesh_channel(nx, ny, Lx, Ly, stretch, block, porosity, block2)
+    mesh = _mesh_channel(nx, ny, Lx, Ly, stretch, block, porosity, block2)
     if dtau is None:
         dtau = stable_dtau(mesh, beta, dt)
     prm = Params(imax=nx, jmax=ny, scheme=scheme, bc=BC_CHANNEL, solve_scalars=int(scalars),
@@ -96,10 +121,10 @@ def channel_case(nx, ny, *, seed=0, case_id=0, Re=100.0, scheme=SCHEME_QUICK, bl
     # u update region i = 3..nx-1, j = 2..ny-1; v update region i = 2..nx-1, j = 3..ny-1;
     # noise index = the Fortran linear index (i-1) + (j-1)*leading dimension
     I, J = np.meshgrid(np.arange(3, nx), np.arange(2, ny), indexing="ij")
-    um[I - 1, J - 1] = noise_array(seed, case_id, NOISE_U, ((I - 1) + (J - 1) * (nx + 1)).ravel(),
+    um[I - 1, J - 1] = _noise_array(seed, case_id, NOISE_U, ((I - 1) + (J - 1) * (nx + 1)).ravel(),
                                    noise_amp).reshape(I.shape)
     I, J = np.meshgrid(np.arange(2, nx), np.arange(3, ny), indexing="ij")
-    vm[I - 1, J - 1] = noise_array(seed, case_id, NOISE_V, ((I - 1) + (J - 1) * nx).ravel(),
+    vm[I - 1, J - 1] = _noise_array(seed, case_id, NOISE_V, ((I - 1) + (J - 1) * nx).ravel(),
                                    noise_amp).reshape(I.shape)
     porous = mesh["flag"] != 0
     st["T"][:] = 1.0
@@ -136,7 +161,7 @@ def cfg_full(n=102, **kw):
 
 
 def uniform01(seed, case_id, k):
-    return 0.5 * (noise(seed, case_id, NOISE_PARAM + k, 0, 1.0) + 1.0)
+    return 0.5 * (_noise(seed, case_id, NOISE_PARAM + k, 0, 1.0) + 1.0)
 
 
 def batch_case_params(case_id, seed=0, sizes=(51, 102, 153, 204)):

@@ -51,14 +51,14 @@ struct LdGen {
   static __device__ __forceinline__ Met met(const double* t, int k) { return met_ldg(t, k); }
 };
 // Everything from shared memory: the tile engine stages the fields and slices of the metric
-// tables (CaseDev::mx/my then point into those slices) before it computes.
+// tables before it computes.  A slice holds the four components of S consecutive table entries
+// one after the other (component c of entry k at t[k + c*S], where CaseDev::mx/my point k0
+// words before a slice that starts at entry k0), so the lanes of a warp, on consecutive columns,
+// read consecutive words.
+template <int S>
 struct LdShared {
   static __device__ __forceinline__ double ld(const double* a, long long q) { return a[q]; }
-  static __device__ __forceinline__ Met met(const double* t, int k) {
-    const double2 a = reinterpret_cast<const double2*>(t)[2 * k];
-    const double2 b = reinterpret_cast<const double2*>(t)[2 * k + 1];
-    return {a.x, a.y, b.x, b.y};
-  }
+  static __device__ __forceinline__ Met met(const double* t, int k) { return {t[k], t[k + S], t[k + 2 * S], t[k + 3 * S]}; }
 };
 
 // QUICK face value seen from the face's upstream side (equations.f90:27-70 rearranged):

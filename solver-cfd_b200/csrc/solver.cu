@@ -557,10 +557,13 @@ int te_setup(Batch& b) {
 
 // one pseudo-iteration of the tile engine: U/V stages 1-3, P + T/C, control
 void te_iteration(Batch& b) {
-  for (int s = 1; s <= 3; ++s) te_launch_uv(s, b.dc, b.dk, b.d_tetiles, b.n_tetiles, b.d_temaps, b.d_te_err, b.stream);
+  for (int s = 1; s <= 3; ++s) {
+    te_launch_uv(s, b.dc, b.dk, b.d_tetiles, b.n_tetiles, b.d_temaps, b.d_te_err, b.stream);
+    if (s == 1) te_launch_tau_bc(b.dc, b.dk, b.n, b.stream);
+  }
   te_launch_ptc(b.dc, b.dk, b.d_tetiles, b.n_tetiles, b.d_temaps, b.d_te_err, b.stream);
   k_control<<<b.n, 256, 0, b.stream>>>(b.dc, b.dk, b.d_iters, b.d_err, b.d_nactive);
-  b.launches += 5;
+  b.launches += 6;
 }
 
 // one pseudo-iteration (main.f90:122-150) for every active case
@@ -711,20 +714,6 @@ int run_graph(Batch& b, int n_steps) {
     if (r) return r;
     b.graph_steps = n_steps;
   }
-  long long pre = 0;
-  if (b.engine == 2) {
-    // After an upload (or a committed warm start) um_tau / vm_tau may not satisfy the boundary
-    // passes, and the reference's first solve_U / solve_V read them before their bcUV side
-    // effects: that iteration runs with the per-stage kernels in the reference's order.
-    bool dirty = false;
-    for (int c = 0; c < b.n; ++c) dirty |= b.hk[c].tau_dirty != 0;
-    if (dirty) {
-      const long long l0 = b.launches;
-      seq_iteration(b);
-      pre = b.launches - l0;
-      CU(cudaMemsetAsync(b.d_nactive, 0, sizeof(int), b.stream));
-    }
-  }
   if (b.graph_conditional) {
     CU(cudaGraphLaunch(b.gexec, b.stream));
     CU(cudaStreamSynchronize(b.stream));
@@ -741,7 +730,7 @@ int run_graph(Batch& b, int n_steps) {
   }
   long long iters_done = 0;
   CU(cudaMemcpy(&iters_done, b.d_iter, sizeof(long long), cudaMemcpyDeviceToHost));
-  b.launches = iters_done * b.body_kernels + pre;
+  b.launches = iters_done * b.body_kernels;
   if (b.engine == 2) {
     int te_err = 0;
     CU(cudaMemcpy(&te_err, b.d_te_err, sizeof(int), cudaMemcpyDeviceToHost));

@@ -25,9 +25,11 @@
 // stencil of an interior node of the next region has its sources within the current region).
 //
 // The first pseudo-iteration after the state was uploaded reads um_tau / vm_tau before their
-// boundary passes (the reference's bcUV side effects); the host runs that iteration with the
-// per-stage kernels of kernels_fast.cu, which follow the reference's order, and this engine from
-// the second iteration on.
+// boundary passes: solve_U's stage 1 reads both as they are, solve_V's stage 1 reads vm_tau after
+// solve_U's bcUV rewrote its boundary, and stages 2 and 3 read both rewritten.  Stage 1 therefore
+// gives V a copy of the vm_tau box with the boundary pass applied (identical to the box once the
+// arrays satisfy the passes), and k_te_tau_bc applies the passes to um_tau / vm_tau before stage 2
+// for the cases that were uploaded.  Every iteration runs the same kernels and arithmetic.
 //
 // TMA: 2-D tensor maps over each case buffer (dims pitch x (ny+1), FP64, no swizzle, zero fill
 // outside), non-multicast loads into 128-byte aligned shared memory, one mbarrier per CTA with the
@@ -39,6 +41,7 @@
 
 #include <algorithm>
 
+#include "bc_exact.cuh"
 #include "points_fast.cuh"
 
 namespace acs {
@@ -298,14 +301,16 @@ __device__ void bc_cell_pass(const CaseDev& d, const Win& w, int pass, bool neum
 
 __device__ __forceinline__ double nanmax(double m, double a) { return (a > m || a != a) ? a : m; }
 
-// Metric-table slices: entries k0 .. k0+n-1 of a case table (4 doubles each) into shared memory,
-// entries outside the table left unset; returns the pointer that indexes the slice like the table.
-__device__ __forceinline__ const double* met_slice(double* sl, const double* table, int k0, int n, int kmax) {
-  for (int e = threadIdx.x; e < 4 * n; e += blockDim.x) {
-    const int k = k0 + (e >> 2);
-    if (k >= 0 && k <= kmax) sl[e] = __ldg(table + 4 * k + (e & 3));
+// Metric-table slice: entries k0 .. k0+N-1 of a case table (4 doubles each) into shared memory,
+// component c of entry k0+m at sl[m + c*N] (entries outside the table left unset); returns the
+// pointer that LdShared<N>::met indexes by table entry.
+template <int N>
+__device__ __forceinline__ const double* met_slice(double* sl, const double* table, int k0, int kmax) {
+  for (int e = threadIdx.x; e < 4 * N; e += blockDim.x) {
+    const int m = e >> 2, c = e & 3, k = k0 + m;
+    if (k >= 0 && k <= kmax) sl[m + c * N] = __ldg(table + 4 * k + c);
   }
-  return sl - 4 * k0;
+  return sl - k0;
 }
 
 // ---- U and V, Runge-Kutta stage ST ------------------------------------------------------------
@@ -315,7 +320,7 @@ __device__ __forceinline__ const double* met_slice(double* sl, const double* tab
 constexpr int MS_UV = 34;  // metric entries i0-1 .. i0+32
 template <int ST>
 constexpr size_t smem_uv() {
-  return (size_t)(ST == 1 ? 3 : 5) * BOX_UV_BYTES + 3 * NT * NT * 8 + NT * (NT + 1) * 8 + 2 * MS_UV * 32;
+  return (size_t)(ST == 1 ? 4 : 5) * BOX_UV_BYTES + 3 * NT * NT * 8 + NT * (NT + 1) * 8 + 2 * MS_UV * 32;
 }
 
 template <int ST>
@@ -340,7 +345,8 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
   double* Pb = Vb + BU * BU;                   // pn box
   double* Ui = ST == 1 ? Ub : Pb + BU * BU;    // stage inputs
   double* Vi = ST == 1 ? Vb : Ui + BU * BU;
-  double* Um = (ST == 1 ? Pb : Vi) + BU * BU;  // um, then the U stage output
+  double* Um = (ST == 1 ? Pb + BU * BU : Vi) + BU * BU;  // um, then the U stage output (stage 1:
+                                                         // after the vm_tau copy for V)
   double* Vm = Um + NT * NT;                   // vm, then the V stage output
   double* Lg = Vm + NT * NT;                   // liga
   double* Tb = Lg + NT * NT;                   // T, rows j0-1 .. j0+31
@@ -367,8 +373,8 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
   }
   load_case(&d, cs + t.c);
   const CaseDev& dg = cs[t.c];
-  const double* mxs = met_slice(Ms, dg.mx, t.i0 - 1, MS_UV, dg.nx + 1);
-  const double* mys = met_slice(Mt, dg.my, t.j0 - 1, MS_UV, dg.ny + 1);
+  const double* mxs = met_slice<MS_UV>(Ms, dg.mx, t.i0 - 1, dg.nx + 1);
+  const double* mys = met_slice<MS_UV>(Mt, dg.my, t.j0 - 1, dg.ny + 1);
   __syncthreads();
   if (threadIdx.x == 0) {
     d.mx = mxs;
@@ -376,9 +382,25 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
   }
   if (!cta_wait(&bar, 0, &flag, err)) return;
 
-  using PS = PtFastT<LdShared>;
+  using PS = PtFastT<LdShared<MS_UV>>;
   const int nx = d.nx, ny = d.ny;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const double* Vs = Vi;  // the vm_tau (stage 1) or stage input V reads with its stencil
+  if (ST == 1 && (t.i0 - 2 <= 1 || t.i0 + NT + 1 >= nx || t.j0 - 2 <= 2 || t.j0 + NT + 1 >= ny)) {
+    // Stage 1 reads vm_tau twice: solve_U as it is (the reference's bcUV then rewrites its
+    // boundary as a side effect), solve_V after that rewrite.  The two differ only right after an
+    // upload; a box that holds v boundary nodes gets a copy with bcUV's v part applied for V, and U
+    // keeps the box as loaded.
+    double* Vc = Pb + BU * BU;
+    for (int q = threadIdx.x; q < BU * BU; q += blockDim.x) Vc[q] = Vb[q];
+    __syncthreads();
+    const Win wc{Vc, t.i0 - 2, t.j0 - 2, BU, BU, BU};
+    bc_v_pass(d, wc, 0);
+    __syncthreads();
+    bc_v_pass(d, wc, 1);
+    __syncthreads();
+    Vs = Vc;
+  }
   double mu = 0.0, mv = 0.0;
 #pragma unroll 1
   for (int r = 0; r < NT / 8; ++r) {
@@ -391,7 +413,7 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
     // interior nodes: no branch separates the two chains
     const double RU = PS::ru_at(d, Ui, Vb, Pb, BU, qs, por, i, j);
     const double T0 = buoy ? Tb[li + (lj + 1) * NT] : 1.0, T1 = buoy ? Tb[li + lj * NT] : 1.0;
-    const double RV = PS::rv_at(d, Ub, Vi, Pb, T0, T1, BU, qs, por, i, j);
+    const double RV = PS::rv_at(d, Ub, Vs, Pb, T0, T1, BU, qs, por, i, j);
     const double ut = Ub[qs], vt = Vb[qs];
     const double ru = ((Um[qo] - ut) + RU * d.dt) * d.dtau;
     const double rv = ((Vm[qo] - vt) + RV * d.dt) * d.dtau;
@@ -421,13 +443,17 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
     block_max_to(&ctl[t.c].res_v, mv);
   }
   __syncthreads();
-  const Win wu{Um, t.i0, t.j0, NT, NT, NT}, wv{Vm, t.i0, t.j0, NT, NT, NT};
-  bc_u_pass(d, wu, 0);
-  bc_v_pass(d, wv, 0);
-  __syncthreads();
-  bc_u_pass(d, wu, 1);
-  bc_v_pass(d, wv, 1);
-  __syncthreads();
+  // boundary passes, only where the tile holds boundary nodes (u: i in {1,2,nx,nx+1} or
+  // j in {1,ny}; v: i in {1,nx} or j in {1,2,ny,ny+1})
+  if (!(t.i0 >= 3 && t.i0 + NT - 1 <= nx - 1 && t.j0 >= 3 && t.j0 + NT - 1 <= ny - 1)) {
+    const Win wu{Um, t.i0, t.j0, NT, NT, NT}, wv{Vm, t.i0, t.j0, NT, NT, NT};
+    bc_u_pass(d, wu, 0);
+    bc_v_pass(d, wv, 0);
+    __syncthreads();
+    bc_u_pass(d, wu, 1);
+    bc_v_pass(d, wv, 1);
+    __syncthreads();
+  }
   double* uo_g = ST == 3 ? d.U[ru_ntau] : d.S[ST - 1];
   double* vo_g = ST == 3 ? d.V[rv_ntau] : d.S[2 + ST - 1];
   for (int r = 0; r < NT / 8; ++r) {
@@ -447,38 +473,50 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
 constexpr int MS_PTC = 38;  // metric entries i0-2 .. i0+35
 constexpr size_t SMEM_PTC2 = 4 * (size_t)BOX_PTC_BYTES + 5 * (size_t)BOX_UV_BYTES + NT * NT * 8 + 2 * MS_PTC * 32;
 
-template <bool IS_C>
-__device__ void te_scalar(const CaseDev& d, const Tile& t, const double* Un, const double* Vn, const double* Z,
-                          const double* Zp, const double* Lg, double* S1, double* S2, double* zo_g, double zin) {
-  using PS = PtFastT<LdShared>;
+// stage ST (1..3) of one scalar (T: IS_C = false, C: IS_C = true) on the tile grown by 3 - ST
+// nodes, then bcZ / bcC there (only where the region holds boundary cells: `edge`)
+template <bool IS_C, int ST>
+__device__ __forceinline__ void scalar_stage(const CaseDev& d, const Tile& t, const double* Un, const double* Vn,
+                                             const double* Z, const double* Zp, const double* Lg, double* S1,
+                                             double* S2, double zin, bool edge) {
+  using PS = PtFastT<LdShared<MS_PTC>>;
+  constexpr int g = 3 - ST, e = NT + 2 * g, o36 = 2 - g, o40 = 4 - g;
+  constexpr int Pz = ST == 1 ? BP : BU;
+  const double* zin_s = ST == 1 ? Z : ST == 2 ? S1 : S2;
+  double* zout = ST == 2 ? S2 : S1;
   const int nx = d.nx, ny = d.ny;
-#pragma unroll 1
-  for (int st = 1; st <= 3; ++st) {
-    const int g = 3 - st, e = NT + 2 * g, o36 = 2 - g, o40 = 4 - g;
-    const double* zin_s = st == 1 ? Z : st == 2 ? S1 : S2;
-    const int Pz = st == 1 ? BP : BU;
-    double* zout = st == 2 ? S2 : S1;
-    for (int q = threadIdx.x; q < e * e; q += blockDim.x) {
-      const int a = q % e, b = q / e;
-      const int i = t.i0 - g + a, j = t.j0 - g + b;
-      if (i >= 2 && i <= nx - 1 && j >= 2 && j <= ny - 1) {
-        const int q36 = (o36 + a) + (o36 + b) * BU, q40 = (o40 + a) + (o40 + b) * BP;
-        const double Rz = PS::template rs_at<IS_C>(d, Un, Vn, BP, q40, zin_s, Pz, st == 1 ? q40 : q36,
-                                                   Lg[q36] != 0.0, i, j);
-        const double zt = Z[q40];
-        const double rr = ((Zp[q36] - zt) + Rz * d.dt) * d.dtau;
-        if (st == 1) zout[q36] = zt + rr;
-        else if (st == 2) zout[q36] = 0.75 * zt + 0.25 * (S1[q36] + rr);
-        else zout[q36] = 1.0 / 3.0 * zt + 2.0 / 3.0 * (S2[q36] + rr);
-      }
+  for (int q = threadIdx.x; q < e * e; q += blockDim.x) {
+    const int a = q % e, b = q / e;
+    const int i = t.i0 - g + a, j = t.j0 - g + b;
+    if (i >= 2 && i <= nx - 1 && j >= 2 && j <= ny - 1) {
+      const int q36 = (o36 + a) + (o36 + b) * BU, q40 = (o40 + a) + (o40 + b) * BP;
+      const double Rz = PS::template rs_at<IS_C>(d, Un, Vn, BP, q40, zin_s, Pz, ST == 1 ? q40 : q36,
+                                                 Lg[q36] != 0.0, i, j);
+      const double zt = Z[q40];
+      const double rr = ((Zp[q36] - zt) + Rz * d.dt) * d.dtau;
+      if (ST == 1) zout[q36] = zt + rr;
+      else if (ST == 2) zout[q36] = 0.75 * zt + 0.25 * (S1[q36] + rr);
+      else zout[q36] = 1.0 / 3.0 * zt + 2.0 / 3.0 * (S2[q36] + rr);
     }
-    __syncthreads();
+  }
+  __syncthreads();
+  if (edge) {
     const Win w{zout + o36 + o36 * BU, t.i0 - g, t.j0 - g, e, e, BU};
     bc_cell_pass(d, w, 0, false, zin);
     __syncthreads();
     bc_cell_pass(d, w, 1, false, zin);
     __syncthreads();
   }
+}
+
+template <bool IS_C>
+__device__ void te_scalar(const CaseDev& d, const Tile& t, const double* Un, const double* Vn, const double* Z,
+                          const double* Zp, const double* Lg, double* S1, double* S2, double* zo_g, double zin,
+                          bool edge) {
+  scalar_stage<IS_C, 1>(d, t, Un, Vn, Z, Zp, Lg, S1, S2, zin, edge);
+  scalar_stage<IS_C, 2>(d, t, Un, Vn, Z, Zp, Lg, S1, S2, zin, edge);
+  scalar_stage<IS_C, 3>(d, t, Un, Vn, Z, Zp, Lg, S1, S2, zin, edge);
+  const int nx = d.nx, ny = d.ny;
   for (int q = threadIdx.x; q < NT * NT; q += blockDim.x) {
     const int a = q % NT, b = q / NT;
     const int i = t.i0 + a, j = t.j0 + b;
@@ -533,8 +571,8 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_ptc(const CaseDev* __restr
   }
   load_case(&d, cs + t.c);
   const CaseDev& dg = cs[t.c];
-  const double* mxs = met_slice(Ms, dg.mx, t.i0 - 2, MS_PTC, dg.nx + 1);
-  const double* mys = met_slice(Mt, dg.my, t.j0 - 2, MS_PTC, dg.ny + 1);
+  const double* mxs = met_slice<MS_PTC>(Ms, dg.mx, t.i0 - 2, dg.nx + 1);
+  const double* mys = met_slice<MS_PTC>(Mt, dg.my, t.j0 - 2, dg.ny + 1);
   __syncthreads();
   if (threadIdx.x == 0) {
     d.mx = mxs;
@@ -543,7 +581,7 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_ptc(const CaseDev* __restr
   if (!cta_wait(&bar, 0, &flag, err)) return;
 
   // P: pn = p + dtau*beta*RP at the interior cells of the tile, then bcP, then store
-  using PS = PtFastT<LdShared>;
+  using PS = PtFastT<LdShared<MS_PTC>>;
   const int nx = d.nx, ny = d.ny;
   double mp = 0.0;
   for (int q = threadIdx.x; q < NT * NT; q += blockDim.x) {
@@ -558,12 +596,17 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_ptc(const CaseDev* __restr
   }
   block_max_to(&ctl[t.c].res_p, mp);
   __syncthreads();
+  // boundary passes only where a region holds boundary cells (i in {1,nx} or j in {1,ny}); the
+  // test uses the largest region, the tile grown by two nodes
+  const bool edge = !(t.i0 - 2 >= 2 && t.i0 + NT + 1 <= nx - 1 && t.j0 - 2 >= 2 && t.j0 + NT + 1 <= ny - 1);
   {
-    const Win w{P0, t.i0, t.j0, NT, NT, NT};
-    bc_cell_pass(d, w, 0, true, 0.0);
-    __syncthreads();
-    bc_cell_pass(d, w, 1, true, 0.0);
-    __syncthreads();
+    if (edge) {
+      const Win w{P0, t.i0, t.j0, NT, NT, NT};
+      bc_cell_pass(d, w, 0, true, 0.0);
+      __syncthreads();
+      bc_cell_pass(d, w, 1, true, 0.0);
+      __syncthreads();
+    }
     double* pn = d.P[rp1];
     for (int q = threadIdx.x; q < NT * NT; q += blockDim.x) {
       const int a = q % NT, b = q / NT;
@@ -572,12 +615,27 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_ptc(const CaseDev* __restr
     }
   }
   if (!scal) return;
-  te_scalar<false>(d, t, Un, Vn, Zt, Tp, Lg, S1, S2, d.T[rt_ntau], d.T_in);
+  te_scalar<false>(d, t, Un, Vn, Zt, Tp, Lg, S1, S2, d.T[rt_ntau], d.T_in, edge);
   __syncthreads();
-  te_scalar<true>(d, t, Un, Vn, Zc, Cp, Lg, S1, S2, d.C[rc_ntau], d.C_in);
+  te_scalar<true>(d, t, Un, Vn, Zc, Cp, Lg, S1, S2, d.C[rc_ntau], d.C_in, edge);
 }
 
 }  // namespace
+
+// The bcUV side effects of the first iteration after an upload: solve_U's boundary passes rewrite
+// vm_tau's boundary, solve_V's rewrite um_tau's (boundary.f90:1-49); stage 1 has read both arrays
+// as they were, stages 2 and 3 read them rewritten.  One block per case; cases whose tau arrays
+// already satisfy the passes (CaseCtl::tau_dirty == 0) are left alone.
+__global__ void k_te_tau_bc(const CaseDev* __restrict__ cs, CaseCtl* __restrict__ ctl) {
+  const CaseCtl& k = ctl[blockIdx.x];
+  if (!k.active || !k.tau_dirty) return;
+  const CaseDev& d = cs[blockIdx.x];
+  bc_uv_block(d, d.U[k.ru[R_TAU]], d.V[k.rv[R_TAU]]);
+}
+
+void te_launch_tau_bc(const CaseDev* cs, CaseCtl* ctl, int ncases, cudaStream_t s) {
+  k_te_tau_bc<<<ncases, 256, 0, s>>>(cs, ctl);
+}
 
 cudaError_t te_prepare() {
   cudaError_t e = cudaFuncSetAttribute(k_te_uv<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_uv<1>());

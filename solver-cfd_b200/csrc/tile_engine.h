@@ -48,6 +48,9 @@ void te_launch_uv(int stage, const CaseDev* cs, CaseCtl* ctl, const Tile* tiles,
                   int* err, cudaStream_t s);
 void te_launch_ptc(const CaseDev* cs, CaseCtl* ctl, const Tile* tiles, int ntiles, const TeMaps* maps, int* err,
                    cudaStream_t s);
+// The bcUV side effects on um_tau / vm_tau after stage 1 of an iteration that follows an upload
+// (cases with CaseCtl::tau_dirty set).
+void te_launch_tau_bc(const CaseDev* cs, CaseCtl* ctl, int ncases, cudaStream_t s);
 // One-time kernel attributes (dynamic shared memory sizes); returns the first error.
 cudaError_t te_prepare();
 

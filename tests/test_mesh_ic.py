@@ -82,3 +82,20 @@ def test_channel_noise_matches_oracle_generator(pkg, orc):
     for j in range(3, ny):
         for i in range(2, nx):
             assert st["vm"][i - 1, j - 1] == orc.noise(4, 2, 2, (i - 1) + (j - 1) * nx, 1e-3)
+
+
+def test_oracle_generators_build_identical_cases(pkg, orc):
+    """The case builders with the oracle's mesh and noise generators (what a run that must not
+    load the package's library uses) give the same cases bit for bit as with the package's own."""
+    a, _ = pkg.configs.cfg_batch(3, seed=101, sizes=(31, 45), arith=pkg.ARITH_FAST)
+    pkg.configs.use_backend(orc)
+    try:
+        b, _ = pkg.configs.cfg_batch(3, seed=101, sizes=(31, 45), arith=pkg.ARITH_FAST)
+    finally:
+        pkg.configs.use_backend(None)
+    for (p1, m1, s1, i1), (p2, m2, s2, i2) in zip(a, b):
+        assert p1 == p2 and i1 == i2
+        for k in m1:
+            assert np.array_equal(np.asarray(m1[k]), np.asarray(m2[k])), k
+        for k in s1:
+            assert np.array_equal(s1[k], s2[k]), k

@@ -147,3 +147,41 @@ def test_tile_engine_needs_fast_arithmetic(gpu):
     g = gpu.Case(prm, mesh)
     with pytest.raises(gpu.AcsError):
         g.set_option(gpu.OPT_ENGINE, TILE)
+
+
+def test_tile_engine_upload_between_steps_changes_nothing(gpu):
+    """A driver that keeps the state on the host downloads every field after a physical step and
+    uploads it before the next.  The upload marks um_tau / vm_tau as possibly not satisfying the
+    boundary passes, and the next iteration follows the reference's order for them -- with the
+    same kernels as every other iteration, so the trajectory is bit-identical to an uninterrupted
+    run (same iteration counts, same fields)."""
+    pkg = gpu
+    items, _ = pkg.configs.cfg_batch(3, seed=7, sizes=(37, 52), arith=pkg.ARITH_FAST, itc_max=4000)
+    itc0 = np.array([x[3] for x in items], np.int32)
+
+    def make():
+        b = pkg.Batch([x[0] for x in items], [x[1] for x in items])
+        b.set_option(pkg.OPT_ENGINE, TILE)
+        for c, x in enumerate(items):
+            b.set_state(c, x[2])
+        return b
+
+    a = make()
+    itc_a, it_a, _, st_a = a.run(3, itc0)
+    b = make()
+    itc = itc0.copy()
+    its = []
+    for k in range(3):
+        states = [b.get_state(c) for c in range(len(items))]
+        for c in range(len(items)):
+            b.set_state(c, states[c])
+        itc, it, _, st = b.run(1, itc)
+        its.append(it[:, 0])
+    assert (st_a == pkg.CASE_DONE).all()
+    assert np.array_equal(np.stack(its, axis=1), it_a) and np.array_equal(itc, itc_a)
+    for c, (prm, *_r) in enumerate(items):
+        x, y = a.get_state(c), b.get_state(c)
+        for k in pkg.FIELDS:
+            assert np.array_equal(mask_dead(k, x[k], prm.bc), mask_dead(k, y[k], prm.bc)), (c, k)
+    a.close()
+    b.close()
