@@ -1,21 +1,26 @@
 """Benchmark: converged physical steps per second of the artificial-compressibility loop.
 
 A bench step is one converged physical step (a pseudo-time loop run to max residual < eps) of
-every case of the workload.  ``value`` is the whole-job throughput in converged physical steps
-per second with the state resident in HBM; ``e2e`` is the same metric through the C ABI with the
-state copied from pinned host buffers before and back after every step.
+every case of the workload; the unit is converged case-steps per second.  ``value`` is the
+whole-job throughput with the state resident in HBM; ``e2e`` is the same steps again through the
+C ABI with the state copied from pinned host buffers before and back after every step.
 
-The default workload, ws-153, is the batched solver with the learned warm start: 16 held-out
-cases at 153 x 153 drawn from the batched configuration's parameter distribution, each step
-started from the best of the plain, extrapolated and learned start (the U-Net inference and the
-start selection are inside the timed region).  The plain GPU path is timed on the same steps
-from the same state and reported beside it (``plain_gpu``).
+The default workload, ws-153, is the learned-warm-start configuration: 64 held-out cases at
+153 x 153 drawn from the batched configuration's parameter distribution (seed 101; the network
+trained on seed 100), the tile engine, FAST arithmetic.  The W warm-up steps run from rest with
+the reference's (plain) start, recording the warm-start history; the K timed steps each start
+from the best of the plain, extrapolated and learned start (the U-Net inference and the start
+selection inside the timed region).  The plain GPU path is timed on the first steps of the same
+window from the same state (``plain_gpu``).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--arith exact|fast]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--engine tile|cluster|graph]
     python bench.py --impl reference ...   # the CPU implementation of the loop on host cores
 
-Warm-start policy options (off by default): --extrap-order 2 (quadratic extrapolated
-candidate), --warm-eps E (residual tolerance of the warm-started cases of each step).
+The reference arm runs the oracle (the C++ restatement of the reference's OpenMP loop; no
+Fortran compiler exists here) on all host cores: for a sample of the workload's cases it runs
+the W warm-up steps and then times the K steps of the same window, every step converged to the
+same tolerance with the reference's start.  Its cases are built with the oracle's own mesh and
+noise generators, so it never loads this package's library.
 
 Multi-GPU (torchrun): each rank runs its own replica of the workload (cases are independent, so
 there is no exchange on the data path); the elapsed time is the max over ranks.
@@ -36,9 +41,9 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     # name: description
-    "ws-153": "batched solver + learned warm start: 16 cases at 153 x 153, Re U[50,500], Da logU[1e-5,1e-2], "
+    "ws-153": "learned warm start: 64 held-out cases at 153 x 153, Re U[50,500], Da logU[1e-5,1e-2], "
               "porosity U[0.3,0.9], Ri U[0,2], random block position (30% area), full equation set, QUICK, "
-              "residual 1e-6; cases seeded apart from the network's training cases",
+              "beta 1, dt 1e-3, residual 1e-6; cases seeded apart from the network's training cases",
     "full-102": "full equation set (u, v, p, T, C), QUICK, porous block 30% (porosity 0.4, Da 1e-3, Cf 0.55), "
                 "Ri 1, Pr 0.7, Sc 1, Re 200, 102 x 102 stretched 2:1 channel, beta 1, dt 1e-3, residual 1e-6",
     "full-204": "as full-102 on a 204 x 204 mesh",
@@ -54,6 +59,11 @@ BYTES_PER_CELL_UPDATE = {"full": 204, "plain": 112}   # each FP64 field read and
 # per-node algorithmic bytes of the timed u-momentum kernel: reads u_in, um, um_tau, vm_tau, pn
 # (5 x 8 B) and the porous mask (1 B), writes u_out (8 B)
 U_KERNEL_BYTES = {"exact": 49, "fast": 41}
+ENGINES = {"cluster": 0, "graph": 1, "tile": 2}
+# per-node algorithmic bytes of one launch of the tile engine's U/V stage kernel (stage 2): reads
+# u_in, v_in, um_tau, vm_tau, pn, um, vm, T (8 x 8 B) and the porous indicator (1 B, as in the
+# fused model), writes u_out, v_out (2 x 8 B)
+TILE_UV_BYTES = 8 * 8 + 1 + 2 * 8
 
 
 def measured_peaks():
@@ -84,22 +94,23 @@ def replica_seed_offset(rank: int) -> int:
     return rank
 
 
-def build_workload(pkg, name, arith, seed_offset=0, max_iters=None):
-    items, kind = _build_workload(pkg, name, arith, seed_offset)
+def build_workload(pkg, name, arith, seed_offset=0, max_iters=None, cases=None):
+    items, kind = _build_workload(pkg, name, arith, seed_offset, cases)
     if max_iters:
         from dataclasses import replace
         items = [(replace(p, itc_max=max_iters),) + tuple(rest) for p, *rest in items]
     return items, kind
 
 
-WS_CASES, WS_N, WS_SEED = 16, 153, 101   # held-out seed (the network trains on seed 100)
+WS_CASES, WS_N, WS_SEED = 64, 153, 101   # held-out seed (the network trains on seed 100)
 
 
-def _build_workload(pkg, name, arith, seed_offset=0):
+def _build_workload(pkg, name, arith, seed_offset=0, cases=None):
     cfg = pkg.configs
     a = pkg.ARITH_FAST if arith == "fast" else pkg.ARITH_EXACT
     if name == "ws-153":
-        items, _ = cfg.cfg_batch(WS_CASES, seed=WS_SEED + 1000 * seed_offset, sizes=(WS_N,), arith=a)
+        n = cases if cases else WS_CASES
+        items, _ = cfg.cfg_batch(n, seed=WS_SEED + 1000 * seed_offset, sizes=(WS_N,), arith=a)
         return items, "full"
     if name == "batch-256":
         items, _ = cfg.cfg_batch(256, seed=seed_offset, arith=a)
@@ -221,7 +232,7 @@ def run_product(args):
     dev = torch.device("cuda", torch.cuda.current_device())
     stream = torch.cuda.current_stream()
     items, kind = build_workload(pkg, args.workload, args.arith, seed_offset=replica_seed_offset(rank),
-                                 max_iters=args.max_iters)
+                                 max_iters=args.max_iters, cases=args.cases)
     if args.workload.startswith("ws-"):
         return run_ws(args, pkg, items, kind, world, rank, dev, stream)
     tuned = None
@@ -234,8 +245,9 @@ def run_product(args):
     eng_used = "graph" if (tuned or {}).get("engine") == 1 else args.engine
     batch = pkg.Batch([x[0] for x in items], [x[1] for x in items])
     batch.set_stream(stream.cuda_stream)
-    batch.set_option(pkg.OPT_ENGINE, 0 if args.engine == "cluster" else 1)
-    batch.set_option(pkg.OPT_STAGED, args.stage)
+    batch.set_option(pkg.OPT_ENGINE, ENGINES[args.engine])
+    if args.engine == "cluster":
+        batch.set_option(pkg.OPT_STAGED, args.stage)
     if tuned:
         import_module(pkg.__name__ + ".autotune").apply(batch, pkg, tuned)
     for c, x in enumerate(items):
@@ -271,10 +283,6 @@ def run_product(args):
     total_iters = int(iters.sum())
     steps_done = n_cases * args.steps
     capped = int(sum((iters[c] >= items[c][0].itc_max - 1).sum() for c in range(n_cases)))
-    if args.record_iterations and rank == 0:
-        with open(args.record_iterations, "w") as f:
-            json.dump({"workload": args.workload, "warmup": args.warmup, "steps": args.steps,
-                       "iterations": iters.tolist()}, f)
     value = steps_done * world / elapsed
 
     peak, peak_kind = measured_peaks()
@@ -288,19 +296,19 @@ def run_product(args):
         per_launch = {"bytes_per_cell_update": b_cu, "launches": launches,
                       "cell_updates_per_launch": cell_updates / max(launches, 1),
                       "ms_per_launch": elapsed * 1e3 / max(launches, 1)}
+    elif eng_used == "tile":
+        ms_u, nodes_u = batch.time_kernel(5, reps=20)
+        b_node = TILE_UV_BYTES
+        kern = "k_te_uv<2> (tile engine, U/V Runge-Kutta stage 2)"
+        achieved = b_node * cells / (ms_u * 1e-3) / 1e9
+        per_launch = {"bytes_per_node": b_node, "nodes_per_launch": cells, "ms_per_launch": ms_u}
     else:
         ms_u, nodes_u = batch.time_kernel(0, reps=50)
         b_node = U_KERNEL_BYTES[args.arith]
         kern = "k_u_stage_%s (u-momentum stage, graph engine)" % args.arith
         achieved = b_node * nodes_u / (ms_u * 1e-3) / 1e9
         per_launch = {"bytes_per_node": b_node, "nodes_per_launch": nodes_u, "ms_per_launch": ms_u}
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "engine_dram_bytes.json")
-    if eng_used == "cluster" and os.path.exists(tfile):
-        with open(tfile) as f:
-            bpcu = json.load(f).get(kind, {}).get("dram_bytes_per_cell_update")
-        if bpcu:
-            traffic = bpcu * cell_updates / max(launches, 1)
+    traffic = None  # DRAM bytes per launch come from ncu (profiles/), not from this run
 
     # end to end through the C ABI with host buffers (pinned): the same steps as the timed region
     e2e_steps = args.steps
@@ -357,8 +365,7 @@ def run_product(args):
                 "cases_per_gpu": n_cases,
                 "cells_per_gpu": cells,
                 "arith": args.arith,
-                "engine": "graph" if (tuned or {}).get("engine") == 1 else args.engine,
-                "staged": args.stage,
+                "engine": eng_used,
                 "launch_shape": tuned,
                 "pseudo_iterations_per_step_mean": total_iters / steps_done,
                 "steps_capped_at_itc_max": capped,
@@ -400,17 +407,17 @@ def run_product(args):
 def _tuned_batch(pkg, items, args, stream):
     from importlib import import_module
     tuned = None
-    if args.launch_shape:
-        t, c_, n_ = (int(v) for v in args.launch_shape.split(","))
-        tuned = {"threads": t, "ctas_per_sm": c_, "nodes_per_cta": n_, "staged": args.stage}
-    elif args.arith == "fast" and args.engine == "cluster":
-        tuned = import_module(pkg.__name__ + ".autotune").tune(pkg, items, use_cache=not args.retune)
+    if args.engine == "cluster":
+        if args.launch_shape:
+            t, c_, n_ = (int(v) for v in args.launch_shape.split(","))
+            tuned = {"threads": t, "ctas_per_sm": c_, "nodes_per_cta": n_, "staged": args.stage}
+        elif args.arith == "fast":
+            tuned = import_module(pkg.__name__ + ".autotune").tune(pkg, items, use_cache=not args.retune)
 
     def make(states=None):
         b = pkg.Batch([x[0] for x in items], [x[1] for x in items])
         b.set_stream(stream.cuda_stream)
-        b.set_option(pkg.OPT_ENGINE, 0 if args.engine == "cluster" else 1)
-        b.set_option(pkg.OPT_STAGED, args.stage)
+        b.set_option(pkg.OPT_ENGINE, ENGINES[args.engine])
         if tuned:
             import_module(pkg.__name__ + ".autotune").apply(b, pkg, tuned)
         for c, x in enumerate(items):
@@ -433,82 +440,63 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
     make, tuned = _tuned_batch(pkg, items, args, stream)
     l2 = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
 
-    # cost-aware cluster sizes: a batched step lasts as long as its slowest case, so each case gets
-    # CTAs in proportion to its pseudo-iterations of the previous step (cluster engine only)
-    # the total stays that of the tuned launch shape; only its distribution over the cases changes
-    # (--balance 2: the CTA slots of the whole GPU, SMs x CTAs per SM, instead)
-    slots = 0
-    if args.balance and tuned and tuned.get("engine", 0) == 0 and args.engine == "cluster":
-        npc = tuned["nodes_per_cta"]
-        for p, *_ in items:
-            k = -(-((p.imax + 1) * (p.jmax + 1)) // npc)
-            slots += max(1, min(k, 16, max(1, (p.jmax + 1) // 4)))
-        if args.balance == 2:
-            slots = max(slots, torch.cuda.get_device_properties(dev).multi_processor_count * tuned.get("ctas_per_sm", 1))
-
-    def balance(batch, its):
-        if slots and its is not None:
-            batch.balance_clusters(its, slots)
-
+    # ---- warm-up: W steps from rest with the reference's start; every step records the fields in
+    # the warm-start history, so the first timed step can extrapolate
     A = make()
     wA = ws.WarmStart(A, H, W, net, norm, extrap_order=args.extrap_order)
     itc = np.array([x[3] for x in items], np.int32)
-    prev_snap = prev_snap2 = None
-    it_last = None
+    hist = []   # states at the start of the last two warm-up steps (the end-to-end pass rebuilds
+                # the same history from them)
+    it_warmup = np.zeros((n_cases, args.warmup), np.int64)
     for w in range(args.warmup):
-        if w == args.warmup - 2 and args.extrap_order == 2:
-            prev_snap2 = [A.get_state(c) for c in range(n_cases)]
-        if w == args.warmup - 1:
-            prev_snap = [A.get_state(c) for c in range(n_cases)]
-        itc, it_last, _, _ = wA.step(itc, "learned", warm_eps=args.warm_eps)
-        balance(A, it_last)
-    it_warm_last = None if it_last is None else np.array(it_last)
+        hist = (hist + [[A.get_state(c) for c in range(n_cases)]])[-2:]
+        wA.features()
+        itc, it, _, _ = wA.step(itc, "plain")
+        it_warmup[:, w] = it
     torch.cuda.synchronize()
     snap = [A.get_state(c) for c in range(n_cases)]
     itc_snap = itc.copy()
 
-    def timed(step_fn, batch, itc):
-        """K steps; returns (elapsed s, iterations [n, K], chosen starts [n, K], engine ms, start ms,
-        launches)."""
-        iters = np.zeros((n_cases, args.steps), np.int64)
-        chosen = np.zeros((n_cases, args.steps), np.int64)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        eng_ms = 0.0
-        launches = 0
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        ev[0].record(stream)
-        for k in range(args.steps):
-            l2.fill_(float(k))
-            itc, it, ch, ms = step_fn(batch, itc)
-            iters[:, k] = it
-            chosen[:, k] = ch
-            eng_ms += ms
-            launches += batch.launch_count()
-        ev[1].record(stream)
-        torch.cuda.synchronize()
-        el = max_over_ranks(ev[0].elapsed_time(ev[1]) / 1e3, world, dev)
-        return el, iters, chosen, eng_ms, launches, itc
-
-    def ws_step(batch, itc, w=wA):
+    def ws_step(w, batch, itc):
         w.features()
         y = w.predict()
         chosen, _ = batch.set_start(y.data_ptr(), 8, w.norm.out_scale.data_ptr(), pkg.POLICY_BEST)
         if args.warm_eps is not None:
             for c in range(n_cases):
                 batch.set_tolerance(c, args.warm_eps if chosen[c] != pkg.START_PLAIN else batch.params[c].eps)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
         itc, it, _, _ = batch.run(1, itc)
-        e1.record(stream)
-        e1.synchronize()
-        balance(batch, it[:, 0])
-        return itc, it[:, 0], chosen, e0.elapsed_time(e1)
+        return itc, it[:, 0], chosen
 
+    # ---- timed: K warm-started steps, the state resident in HBM
+    iters_ws = np.zeros((n_cases, args.steps), np.int64)
+    chosen_ws = np.zeros((n_cases, args.steps), np.int64)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    launches = 0
+    if world > 1:
+        dist.barrier()
+    itc = itc_snap.copy()
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
-        el_ws, it_ws, ch_ws, eng_ms, launches, _ = timed(ws_step, A, itc_snap.copy())
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for k in range(args.steps):
+            l2.fill_(float(k))
+            itc, it, ch = ws_step(wA, A, itc)
+            iters_ws[:, k] = it
+            chosen_ws[:, k] = ch
+            launches += A.launch_count()
+            ev[k + 1].record(stream)
+        torch.cuda.synchronize()
+    el_ws = max_over_ranks(ev[0].elapsed_time(ev[-1]) / 1e3, world, dev)
+    step_s = [ev[k].elapsed_time(ev[k + 1]) / 1e3 for k in range(args.steps)]
+    ws_state = [A.get_state(c, ("um", "vm", "pn", "T", "C")) for c in range(n_cases)]
+
+    # the dominant kernel, timed alone on the live state (CUDA events on the batch's stream)
+    roof_kernel = {"tile": 5, "graph": 0}.get(args.engine)
+    k_ms = k_nodes = None
+    if roof_kernel is not None:
+        k_ms, k_nodes = A.time_kernel(roof_kernel, reps=20)
     A.close()
+
     # network inference alone, timed on the same canvas (FLOPs of the 15 convolutions)
     x_in = net.input_buffer(n_cases, H, W)
     for _ in range(2):
@@ -524,32 +512,15 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
     fwd_flops = unet.conv_flops(H, W) * n_cases
     del x_in
 
-    # plain GPU path, same steps from the same state: all K steps in one persistent launch, each
-    # case advancing through its steps on its own
-    B = make(snap)
-    balance(B, it_warm_last)
-    if world > 1:
-        dist.barrier()
-    l2.fill_(-1.0)
-    torch.cuda.synchronize()
-    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    p0.record(stream)
-    _, it_pl, _, _ = B.run(args.steps, itc_snap.copy())
-    p1.record(stream)
-    torch.cuda.synchronize()
-    el_pl = max_over_ranks(p0.elapsed_time(p1) / 1e3, world, dev)
-    it_pl = np.asarray(it_pl, np.int64)
-    plain_state = [B.get_state(c, ("um", "vm", "pn", "T", "C")) for c in range(n_cases)]
-    B.close()
-
-    # end to end through the C ABI with pinned host buffers: the same steps again
-    C_ = make(prev_snap2 if prev_snap2 is not None else prev_snap)
-    balance(C_, it_warm_last)
+    # ---- end to end through the C ABI with pinned host buffers: the same K steps again, every
+    # field uploaded before and downloaded after each step
+    C_ = make(hist[0] if hist else None)
     wC = ws.WarmStart(C_, H, W, net, norm, extrap_order=args.extrap_order)
-    wC.features()                       # history: the fields at the start of the last warm-up step
-    if prev_snap2 is not None:          # (and of the one before, for the quadratic candidate)
+    for h in hist[1:]:
+        wC.features()
         for c in range(n_cases):
-            C_.set_state(c, prev_snap[c])
+            C_.set_state(c, h[c])
+    if hist:
         wC.features()
     host = []
     h2d = d2h = 0
@@ -572,58 +543,45 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
     for k in range(args.steps):
         for c in range(n_cases):
             C_.set_state(c, {nme: v for nme, (t, v) in host[c].items()})
-        itc, it, _, _ = ws_step(C_, itc, wC)
+        itc, it, _ = ws_step(wC, C_, itc)
         it_e2e[:, k] = it
         for c in range(n_cases):
             C_.get_state(c, out={nme: v for nme, (t, v) in host[c].items()})
     torch.cuda.synchronize()
-    e2e_el = time.perf_counter() - t0
-    ws_state = [{k: host[c][k][1] for k in ("um", "vm", "pn", "T", "C")} for c in range(n_cases)]
+    e2e_el = max_over_ranks(time.perf_counter() - t0, world, dev)
     C_.close()
-    e2e_el = max_over_ranks(e2e_el, world, dev)
-    err = {}
-    for c in range(n_cases):
-        for k, v in ws.field_error(ws_state[c], plain_state[c]).items():
-            err[k] = max(err.get(k, 0.0), v)
 
-    # kernels of the warm start per step: history, scale, features; input normalisation; the
-    # network (im2col + GEMM per convolution, pool/upsample/skip copy per level); candidates,
-    # boundary passes, residual probes, commit
-    n_unet = 2 * len(net.convs) + 3 * (net.levels - 1)
-    ws_launches = args.steps * (3 + 1 + n_unet + 8)
+    # ---- plain GPU path on the first m steps of the window from the same state, one launch
+    m = max(1, min(args.steps, args.plain_steps))
+    B = make(snap)
+    if world > 1:
+        dist.barrier()
+    l2.fill_(-1.0)
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    _, it_pl, _, _ = B.run(m, itc_snap.copy())
+    p1.record(stream)
+    torch.cuda.synchronize()
+    el_pl = max_over_ranks(p0.elapsed_time(p1) / 1e3, world, dev)
+    it_pl = np.asarray(it_pl, np.int64)
+    plain_state = [B.get_state(c, ("um", "vm", "pn", "T", "C")) for c in range(n_cases)] if m == args.steps else None
+    B.close()
+
     steps_done = n_cases * args.steps
     value = steps_done * world / el_ws
-    plain_value = steps_done * world / el_pl
+    plain_value = n_cases * m * world / el_pl
+    warm_m_value = n_cases * m * world / max_over_ranks(sum(step_s[:m]), world, dev)
     peak, peak_kind = measured_peaks()
     b_cu = BYTES_PER_CELL_UPDATE[kind]
-    cells = items[0][0].imax * items[0][0].jmax
-    cu_ws = int(it_ws.sum()) * cells
-    cu_pl = int(it_pl.sum()) * cells
-    eng_gbs = b_cu * cu_ws / (eng_ms * 1e-3) / 1e9
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "engine_dram_bytes.json")
-    if os.path.exists(tfile):
-        with open(tfile) as f:
-            bpcu = json.load(f).get(kind, {}).get("dram_bytes_per_cell_update")
-        if bpcu:
-            traffic = bpcu * cu_ws / max(launches, 1)
-    bf16_peak = None
+    cells = sum(x[0].imax * x[0].jmax for x in items)
+    cu_ws = int(sum(iters_ws[c].sum() * items[c][0].imax * items[c][0].jmax for c in range(n_cases)))
+    loop_gbs = b_cu * cu_ws / el_ws / 1e9
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             bf16_peak = float(json.load(f)["bf16_tflops"])
     except (OSError, KeyError, ValueError):
         bf16_peak = 1590.0
-    if args.record_iterations and rank == 0:
-        rec = {}
-        if os.path.exists(args.record_iterations):
-            with open(args.record_iterations) as f:
-                rec = json.load(f)
-        rec[args.workload] = {"warmup": args.warmup, "steps": args.steps,
-                              "plain_iterations": it_pl.tolist(),
-                              "mean_iterations_per_step": [float(v) for v in it_pl.mean(axis=1)],
-                              "warm_start_iterations": it_ws.tolist()}
-        with open(args.record_iterations, "w") as f:
-            json.dump(rec, f, indent=1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import oracle as orc
@@ -631,7 +589,22 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
         state_items = [(x[0], x[1], snap[c], 0) for c, x in enumerate(items)]
         cpu = cpu_sample(orc, state_items, gips, budget_s=args.cpu_seconds)
     if rank == 0:
-        starts = np.bincount(ch_ws.ravel(), minlength=3) / ch_ws.size
+        starts = np.bincount(chosen_ws.ravel(), minlength=3) / chosen_ws.size
+        if k_ms is not None:
+            kname = ("k_te_uv<2> (tile engine, U/V Runge-Kutta stage 2)" if args.engine == "tile"
+                     else "k_u_stage (graph engine, u-momentum stage 1)")
+            b_node = TILE_UV_BYTES if args.engine == "tile" else U_KERNEL_BYTES[args.arith]
+            nodes = cells if args.engine == "tile" else k_nodes
+            achieved = b_node * nodes / (k_ms * 1e-3) / 1e9
+            roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                    "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst)" if peak_kind == "measured" else "fallback",
+                    "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                    "bytes_per_node": b_node, "nodes_per_launch": nodes, "ms_per_launch": k_ms,
+                    "traffic_note": "DRAM bytes per launch are measured by ncu (profiles/), not inside this run"}
+        else:
+            roof = {"bound": "hbm", "kernel": "k_engine (persistent cluster engine)", "achieved": loop_gbs,
+                    "peak": peak, "unit": "GB/s", "frac": loop_gbs / peak, "traffic": None,
+                    "bytes_per_cell_update": b_cu}
         line = {
             "metric": "converged physical steps/s at pseudo-time residual 1e-6",
             "value": value,
@@ -649,101 +622,102 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
                 "workload": args.workload,
                 "description": WORKLOADS[args.workload],
                 "cases_per_gpu": n_cases,
-                "cells_per_gpu": cells * n_cases,
+                "cells_per_gpu": cells,
                 "arith": args.arith,
-                "engine": "graph" if (tuned or {}).get("engine") == 1 else args.engine,
-                "staged": args.stage,
+                "engine": args.engine,
                 "launch_shape": tuned,
                 "network": {"weights": os.path.relpath(args.weights, ROOT), "canvas": [H, W],
                             "trained_snapshots": meta.get("snapshots")},
-                "pseudo_iterations_per_step_mean": float(it_ws.mean()),
+                "warmup_start": "plain (the reference's start), recording the warm-start history",
+                "pseudo_iterations_per_step_mean": float(iters_ws.mean()),
+                "pseudo_iterations_per_step_slowest_case_mean": float(iters_ws.max(axis=0).mean()),
+                "warmup_pseudo_iterations_per_step_mean": it_warmup.mean(axis=0).round(1).tolist(),
                 "starts_plain_extrap_learned": starts.round(3).tolist(),
                 "warm_start_tolerance": args.warm_eps if args.warm_eps is not None else "each case's own (1e-6)",
                 "extrapolation_order": args.extrap_order,
-                "cluster_sizes": ("the launch shape's CTAs redistributed in proportion to each case's pseudo-"
-                                  f"iterations of the previous step, {slots} CTAs in total (plain run: by the "
-                                  "last warm-up step)") if slots
-                                 else "from the launch shape",
                 "l2": "flushed (256 MB write) before every timed step",
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             },
-            "plain_gpu": {"value": plain_value, "unit": "steps/s", "ms_per_step": el_pl / args.steps * 1e3,
-                          "launch": "acs_batch_run over all timed steps in one launch (no per-step host sync)",
+            "plain_gpu": {"value": plain_value, "unit": "steps/s", "steps": m, "ms_per_step": el_pl / m * 1e3,
+                          "launch": f"acs_batch_run over the first {m} timed steps in one launch",
                           "pseudo_iterations_per_step_mean": float(it_pl.mean()),
-                          "speedup_of_warm_start": value / plain_value,
-                          "final_fields_max_rel_diff_warm_vs_plain": err},
+                          "warm_start_value_same_steps": warm_m_value,
+                          "speedup_of_warm_start": warm_m_value / plain_value,
+                          "warm_pseudo_iterations_per_step_mean_same_steps": float(iters_ws[:, :m].mean()),
+                          "final_fields_max_rel_diff_warm_vs_plain": (
+                              {k: max(ws.field_error(ws_state[c], plain_state[c])[k] for c in range(n_cases))
+                               for k in ("um", "vm", "pn", "T", "C")} if plain_state is not None else None)},
             "cell_updates_per_s": cu_ws * world / el_ws,
-            "roofline": {
-                "bound": "hbm",
-                "kernel": ("pseudo-time loop of the graph engine (per-stage kernels, %s arithmetic)" % args.arith
-                           if (tuned or {}).get("engine") == 1 else
-                           "k_engine (persistent cluster engine, %s arithmetic)" % args.arith),
-                "achieved": eng_gbs,
-                "peak": peak,
-                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst)" if peak_kind == "measured" else "fallback",
-                "unit": "GB/s",
-                "frac": eng_gbs / peak,
-                "traffic": traffic,
-                "bytes_per_cell_update": b_cu,
-                "launches": launches,
-                "ms_per_launch": eng_ms / max(launches, 1),
-                "engine_share_of_step": eng_ms * 1e-3 / el_ws,
-            },
+            "roofline": roof,
+            "loop_roofline": {"bytes_per_cell_update": b_cu, "achieved": loop_gbs, "unit": "GB/s",
+                              "frac": loop_gbs / peak,
+                              "note": "fused-kernel model bytes x cell-updates / whole timed region"},
             "unet_inference": {"bound": "tensor", "flops_per_launch_set": fwd_flops, "ms": fwd_ms,
                                "achieved_tflops": fwd_flops / (fwd_ms * 1e-3) / 1e12,
                                "peak_tflops": bf16_peak, "frac": fwd_flops / (fwd_ms * 1e-3) / 1e12 / bf16_peak},
             "e2e": {"value": n_cases * args.steps * world / e2e_el, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": args.steps,
-                    "same_iterations_as_timed": bool((it_e2e == it_ws).all())},
-            "gpu_launches": launches + ws_launches,
-            "gpu_launches_detail": {"engine": launches, "warm_start_and_network": ws_launches},
+                    "same_iterations_as_timed": bool((it_e2e == iters_ws).all())},
+            "gpu_launches": launches,
             "clocks": clk.summary(),
         }
         if cpu is not None:
             line["cpu_baseline"] = {"value": cpu["steps_per_s"], "unit": "steps/s", "cores": cpu["cores"],
-                                    "kind": "port", "sample": cpu["sample"] + " (plain start's iteration counts)"}
+                                    "kind": "port",
+                                    "sample": cpu["sample"] + f" (plain start's counts of the first {m} steps)"}
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
 
 
-def reference_iterations(workload):
-    path = os.path.join(ROOT, "tests", "golden", "bench_iterations.json")
+def _oracle_items(args):
+    """The workload's cases built with the oracle's mesh and noise generators (this package's
+    Python case builders, no call into its library)."""
+    import __graft_entry__ as entry
+    from oracle import oracle as orc
+    pkg = entry.load_package()
+    pkg.configs.use_backend(orc)
     try:
-        with open(path) as f:
-            return json.load(f).get(workload)
-    except (OSError, ValueError):
-        return None
+        items, kind = build_workload(pkg, args.workload, "exact", max_iters=args.max_iters, cases=args.cases)
+    finally:
+        pkg.configs.use_backend(None)
+    return items, kind
 
 
 def run_reference(args):
-    """The reference's CPU implementation of the loop (the oracle restatement: the Fortran
-    reference cannot be compiled without a Fortran compiler) on the host cores."""
+    """The reference's CPU implementation of the loop on the host cores: the oracle, a C++
+    restatement of OpenMp_Multicore/main.f90:116-186 and equations.f90 (the Fortran sources
+    cannot be compiled here), in the reference's operation order with OpenMP over all host
+    threads.  For `--ref-cases` cases of the workload (spread over its case ids) it runs the W
+    warm-up steps from rest and then times the K steps of the window, every step converged with
+    the reference's start; value = converged case-steps / seconds."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import numpy as np
-    import __graft_entry__ as entry
     from oracle import oracle as orc
-    pkg = entry.load_package()
-    items, kind = build_workload(pkg, args.workload, args.arith, max_iters=args.max_iters)
-    rec = reference_iterations(args.workload)
-    if rec is None:
-        print(json.dumps({"impl": "reference", "unavailable": "tests/golden/bench_iterations.json lacks "
-                          f"pseudo-iteration counts for workload {args.workload}"}))
-        return
-    per_case = rec["mean_iterations_per_step"]
-    gips = per_case if isinstance(per_case, list) else [per_case] * len(items)
-    vals = []
-    t0 = time.perf_counter()
-    cpu = None
-    for k in range(args.warmup + args.steps):
-        cpu = cpu_sample(orc, items, gips, budget_s=max(2.0, args.cpu_seconds / max(1, args.steps)))
-        if k >= args.warmup:
-            vals.append(cpu["steps_per_s"])
-    value = statistics.mean(vals)
-    elapsed = time.perf_counter() - t0
+    items, kind = _oracle_items(args)
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    n = len(items)
+    ns = max(1, min(args.ref_cases, n))
+    picks = sorted({int(round(q * (n - 1) / max(1, ns - 1))) for q in range(ns)}) if ns > 1 else [0]
+    t_all = time.perf_counter()
+    secs = 0.0
+    iters = {}
+    for c in picks:
+        prm, mesh, st, itc = items[c]
+        o = orc.OracleCase(prm, mesh)
+        s = {k: np.asfortranarray(v.copy()) for k, v in st.items()}
+        if args.warmup:
+            itc, _, _ = o.run(s, args.warmup, itc)
+        t0 = time.perf_counter()
+        itc, it, _ = o.run(s, args.steps, itc)
+        secs += time.perf_counter() - t0
+        iters[str(c)] = [int(v) for v in it]
+    wall = time.perf_counter() - t_all
+    value = len(picks) * args.steps / secs
     line = {
         "impl": "reference",
         "metric": "converged physical steps/s at pseudo-time residual 1e-6",
@@ -752,19 +726,21 @@ def run_reference(args):
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": 1e3 / value,
+        "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded channel cases; no public dataset)",
-        "config": {"workload": args.workload, "description": WORKLOADS[args.workload], "cases": len(items),
-                   "pseudo_iterations_per_step_mean": float(np.mean(gips)),
-                   "source_of_iteration_counts": "tests/golden/bench_iterations.json"},
-        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cpu["cores"], "kind": "port",
-                         "sample": cpu["sample"] + " (initial state of the workload)"},
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload], "cases": n,
+                   "sampled_cases": picks, "pseudo_iterations_per_step": iters,
+                   "start": "the reference's (plain) start in every step, warm-up included"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
+                         "sample": f"cases {picks} of the {n}: {args.warmup} warm-up steps from rest, then "
+                                   f"{args.steps} timed converged steps each, one case at a time on all "
+                                   f"{threads} host threads"},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "wall_s": elapsed,
+        "wall_s": wall,
     }
     print(json.dumps(line))
 
@@ -772,22 +748,21 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--workload", default="ws-153", choices=sorted(WORKLOADS))
     ap.add_argument("--weights", default=os.path.join(ROOT, "solver-cfd_b200", "unet", "weights", "ws_153.npz"),
                     help="trained warm-start network (ws-* workloads)")
     ap.add_argument("--arith", default="fast", choices=["exact", "fast"])
-    ap.add_argument("--engine", default="cluster", choices=["cluster", "graph"])
-    ap.add_argument("--retune", action="store_true", help="ignore the autotuner cache")
+    ap.add_argument("--engine", default="tile", choices=sorted(ENGINES))
+    ap.add_argument("--retune", action="store_true", help="ignore the autotuner cache (cluster engine)")
     ap.add_argument("--launch-shape", default=None,
-                    help="threads,ctas_per_sm,nodes_per_cta: skip the autotuner (profiling runs)")
+                    help="cluster engine: threads,ctas_per_sm,nodes_per_cta (skip the autotuner)")
     ap.add_argument("--stage", type=int, default=1, choices=[0, 1],
-                    help="FAST engine: stage stencil arrays in shared memory (1) or read them from L1/L2 (0)")
-    ap.add_argument("--balance", type=int, default=1, choices=[0, 1, 2],
-                    help="ws-* workloads: cluster sizes in proportion to each case's pseudo-iterations "
-                         "(1: within the tuned shape's CTA total, 2: within all CTA slots of the GPU)")
+                    help="cluster engine: stage stencil arrays in shared memory (1) or read them from L1/L2 (0)")
+    ap.add_argument("--plain-steps", type=int, default=3,
+                    help="ws-* workloads: steps of the window on which the plain GPU path is timed")
     ap.add_argument("--extrap-order", type=int, default=1, choices=[1, 2],
                     help="warm-start workload: linear (1) or quadratic (2) extrapolated candidate")
     ap.add_argument("--warm-eps", type=float, default=None,
@@ -795,11 +770,13 @@ def main():
                          "(default: every case keeps its own, 1e-6)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-cases", type=int, default=2,
+                    help="reference arm: cases of the workload run on the CPU (spread over the case ids)")
+    ap.add_argument("--cases", type=int, default=None,
+                    help="ws-* workloads: number of cases (default: the configuration's 64)")
     ap.add_argument("--max-iters", type=int, default=None,
                     help="cap the pseudo-iterations of every physical step (profiling runs; the steps "
                          "are then not converged)")
-    ap.add_argument("--record-iterations", default=None,
-                    help="write the per-step pseudo-iteration counts of the run to this JSON file")
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1:
         raise SystemExit("bad --steps/--warmup")
