@@ -62,4 +62,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python make_golden.py <root of the reference project checkout>")
+    main(sys.argv[1])

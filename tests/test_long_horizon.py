@@ -1,0 +1,89 @@
+"""Long runs of the benchmark configurations: parity after many physical steps.
+
+Short runs cannot show that the FAST arithmetic keeps the reference's iteration counts: the exit
+test (main.f90:142) is discontinuous, so one extra pseudo-iteration late in a long run would show
+up as a different count and fields that drift apart.  These tests run whole trajectories.
+
+* cfg1 (plain method, 51 x 51, upwind, 200 physical steps from rest): the GPU against the oracle's
+  own 200-step run (tests/golden/cfg1_plain51_200.npz, made by make_long_goldens.py).  The EXACT
+  arithmetic is bit-identical; the FAST arithmetic of the tile engine (the benchmark's path) keeps
+  every step's iteration count and stays within 1e-10 relative max-norm per field.
+* cfg2 (full equation set, QUICK, porous block, buoyancy, T and C, 102 x 102) and one 153 x 153
+  case of the learned-warm-start configuration: the FAST tile engine against the EXACT cluster
+  engine on the same device (the EXACT engine is bit-identical to the oracle in the per-routine
+  and whole-loop tests; the oracle itself would need hours for these runs), identical per-step
+  iteration counts and fields within 1e-10.  The step counts are stated in each test.
+"""
+import os
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+FIELDS = ("um", "vm", "p", "pn", "um_tau", "vm_tau")
+FULL = FIELDS + ("T", "C", "T_tau", "C_tau")
+
+
+def _rel(x, y):
+    return float(np.abs(x - y).max() / max(np.abs(y).max(), 1e-300))
+
+
+def _run(pkg, prm, mesh, st, itc, nsteps, engine, arith):
+    g = pkg.Case(replace(prm, arith=arith), mesh)
+    g.set_option(pkg.OPT_ENGINE, engine)
+    g.set_state(st)
+    itc_g, it_g, _, status = g.physical_steps(nsteps, itc)
+    assert status == pkg.CASE_DONE
+    out = g.get_state()
+    g.close()
+    return itc_g, np.asarray(it_g, np.int64), out
+
+
+@pytest.mark.parametrize("engine,arith", [(0, 0), (2, 1)], ids=["cluster-exact", "tile-fast"])
+def test_cfg1_200_steps_against_oracle(gpu, engine, arith):
+    pkg = gpu
+    ref = np.load(os.path.join(GOLDEN, "cfg1_plain51_200.npz"))
+    prm, mesh, st, itc, nsteps = pkg.configs.cfg_plain()
+    assert nsteps == 200 == ref["iterations"].size
+    itc_g, it_g, out = _run(pkg, prm, mesh, st, itc, nsteps, engine, arith)
+    assert np.array_equal(it_g, ref["iterations"]), np.flatnonzero(it_g != ref["iterations"])[:10]
+    assert itc_g == int(ref["itc"])
+    worst = max(_rel(out[k], ref[k]) for k in FIELDS)
+    print(f"cfg1 {'exact' if arith == 0 else 'fast'}: {int(it_g.sum())} pseudo-iterations, "
+          f"max rel diff {worst:.3e}")
+    if arith == 0:
+        for k in FIELDS:
+            assert np.array_equal(out[k], ref[k]), k
+    else:
+        assert worst < TOL
+
+
+def _fast_vs_exact(pkg, prm, mesh, st, itc, nsteps, label):
+    itc_e, it_e, out_e = _run(pkg, prm, mesh, st, itc, nsteps, 0, pkg.ARITH_EXACT)
+    itc_f, it_f, out_f = _run(pkg, prm, mesh, st, itc, nsteps, 2, pkg.ARITH_FAST)
+    diff = np.flatnonzero(it_e != it_f)
+    assert diff.size == 0 and itc_e == itc_f, (label, diff[:10], it_e[diff[:10]], it_f[diff[:10]])
+    worst = {k: _rel(out_f[k], out_e[k]) for k in FULL}
+    print(f"{label}: {nsteps} steps, {int(it_e.sum())} pseudo-iterations, max rel diff per field "
+          + ", ".join(f"{k} {v:.2e}" for k, v in worst.items()))
+    assert max(worst.values()) < TOL, worst
+
+
+def test_cfg2_102_fast_tile_against_exact(gpu):
+    """cfg2 at 102 x 102: 60 physical steps from the seeded start (the first steps are the
+    costliest, up to ~10^5 pseudo-iterations each)."""
+    prm, mesh, st, itc, _ = gpu.configs.cfg_full(102)
+    _fast_vs_exact(gpu, prm, mesh, st, itc, 60, "cfg2 102x102")
+
+
+def test_ws153_case_fast_tile_against_exact(gpu):
+    """One 153 x 153 case of the learned-warm-start configuration (held-out seed 101, case 0):
+    8 physical steps from rest, each converged (several 10^5 pseudo-iterations per step)."""
+    items, _ = gpu.configs.cfg_batch(1, seed=101, sizes=(153,))
+    prm, mesh, st, itc = items[0]
+    _fast_vs_exact(gpu, prm, mesh, st, itc, 8, "ws-153 case 0")
