@@ -12,7 +12,8 @@ up as a different count and fields that drift apart.  These tests run whole traj
   case of the learned-warm-start configuration: the FAST tile engine against the EXACT cluster
   engine on the same device (the EXACT engine is bit-identical to the oracle in the per-routine
   and whole-loop tests; the oracle itself would need hours for these runs), identical per-step
-  iteration counts and fields within 1e-10.  The step counts are stated in each test.
+  iteration counts and fields within 1e-10.  Their step counts default to short runs that keep
+  the GPU suite within minutes; ACS_CFG2_STEPS and ACS_WS153_STEPS set longer ones.
 """
 import os
 from dataclasses import replace
@@ -75,15 +76,16 @@ def _fast_vs_exact(pkg, prm, mesh, st, itc, nsteps, label):
 
 
 def test_cfg2_102_fast_tile_against_exact(gpu):
-    """cfg2 at 102 x 102: 60 physical steps from the seeded start (the first steps are the
-    costliest, up to ~10^5 pseudo-iterations each)."""
+    """cfg2 at 102 x 102: the first physical steps from the seeded start, 20 by default (the
+    first steps are the costliest, up to ~10^5 pseudo-iterations each)."""
     prm, mesh, st, itc, _ = gpu.configs.cfg_full(102)
-    _fast_vs_exact(gpu, prm, mesh, st, itc, 60, "cfg2 102x102")
+    _fast_vs_exact(gpu, prm, mesh, st, itc, int(os.environ.get("ACS_CFG2_STEPS", "20")), "cfg2 102x102")
 
 
 def test_ws153_case_fast_tile_against_exact(gpu):
-    """One 153 x 153 case of the learned-warm-start configuration (held-out seed 101, case 0):
-    8 physical steps from rest, each converged (several 10^5 pseudo-iterations per step)."""
+    """One 153 x 153 case of the learned-warm-start configuration (held-out seed 101, case 0): the
+    first physical steps from rest, 3 by default, each converged (several 10^5 pseudo-iterations
+    per step)."""
     items, _ = gpu.configs.cfg_batch(1, seed=101, sizes=(153,))
     prm, mesh, st, itc = items[0]
-    _fast_vs_exact(gpu, prm, mesh, st, itc, 8, "ws-153 case 0")
+    _fast_vs_exact(gpu, prm, mesh, st, itc, int(os.environ.get("ACS_WS153_STEPS", "3")), "ws-153 case 0")
