@@ -76,16 +76,16 @@ def _fast_vs_exact(pkg, prm, mesh, st, itc, nsteps, label):
 
 
 def test_cfg2_102_fast_tile_against_exact(gpu):
-    """cfg2 at 102 x 102: the first physical steps from the seeded start, 20 by default (the
+    """cfg2 at 102 x 102: the first physical steps from the seeded start, 4 by default (the
     first steps are the costliest, up to ~10^5 pseudo-iterations each)."""
     prm, mesh, st, itc, _ = gpu.configs.cfg_full(102)
-    _fast_vs_exact(gpu, prm, mesh, st, itc, int(os.environ.get("ACS_CFG2_STEPS", "20")), "cfg2 102x102")
+    _fast_vs_exact(gpu, prm, mesh, st, itc, int(os.environ.get("ACS_CFG2_STEPS", "4")), "cfg2 102x102")
 
 
 def test_ws153_case_fast_tile_against_exact(gpu):
     """One 153 x 153 case of the learned-warm-start configuration (held-out seed 101, case 0): the
-    first physical steps from rest, 3 by default, each converged (several 10^5 pseudo-iterations
+    first physical steps from rest, 1 by default, each converged (several 10^5 pseudo-iterations
     per step)."""
     items, _ = gpu.configs.cfg_batch(1, seed=101, sizes=(153,))
     prm, mesh, st, itc = items[0]
-    _fast_vs_exact(gpu, prm, mesh, st, itc, int(os.environ.get("ACS_WS153_STEPS", "3")), "ws-153 case 0")
+    _fast_vs_exact(gpu, prm, mesh, st, itc, int(os.environ.get("ACS_WS153_STEPS", "1")), "ws-153 case 0")
