@@ -589,7 +589,10 @@ int build_graph(Batch& b, int n_steps) {
   if (b.gexec) { cudaGraphExecDestroy(b.gexec); b.gexec = nullptr; }
   if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
   const long long saved = b.launches;
-  if (b.graph_conditional && !getenv("ACS_NO_CONDITIONAL_GRAPH")) {
+  // ACS_NO_CONDITIONAL_GRAPH=1 selects the host-polled loop below (profilers cannot look inside
+  // a graph that holds conditional nodes)
+  if (getenv("ACS_NO_CONDITIONAL_GRAPH")) b.graph_conditional = false;
+  if (b.graph_conditional) {
     cudaGraph_t g;
     CU(cudaGraphCreate(&g, 0));
     cudaGraphConditionalHandle h;
