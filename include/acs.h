@@ -200,7 +200,15 @@ int acs_solve_u_static(const acs_params* p, const acs_grid* grid_dev, const doub
 enum acs_option {
   ACS_OPT_ENGINE = 1,        /* 0 (default): persistent cluster engine, one thread-block cluster
                                 per case runs whole physical steps in one launch;
-                                1: CUDA graph of per-stage kernels with a device WHILE node */
+                                1: CUDA graph of per-stage kernels with a device WHILE node;
+                                2: tile engine, ACS_ARITH_FAST only (ACS_E_UNSUPPORTED otherwise):
+                                   32 x 32-node tiles of every active case loaded into shared
+                                   memory by TMA, four kernels per pseudo-iteration in a CUDA graph
+                                   with a device WHILE node -- the fastest for many cases.  Setting
+                                   it builds the tile table and tensor maps (device memory).  With
+                                   the environment variable ACS_NO_CONDITIONAL_GRAPH set, engines 1
+                                   and 2 loop from the host instead (one graph launch per
+                                   pseudo-iteration), which profilers can look inside */
   ACS_OPT_NODES_PER_CTA = 2, /* engine: target nodes per CTA when sizing a case's cluster */
   ACS_OPT_L1_LOADS = 3,      /* FAST engine: 1 (default) reads cluster-written arrays through L1 */
   ACS_OPT_THREADS = 4,       /* FAST engine: threads per CTA, 256 or 512 (default) */
