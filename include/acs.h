@@ -115,6 +115,16 @@ int acs_mesh_reference(int imax, double porosity, double* x, double* y, double* 
 int acs_mesh_channel(int imax, int jmax, double Lx, double Ly, double s, const double* box1,
                      const double* box2, double porosity, double* x, double* y, double* xm,
                      double* ym, int* flag, double* epsilon1, double* liga_poros);
+/* acs_mesh_channel generated on the device, for batches of synthetic cases built without host
+ * arrays (no reference counterpart beyond nonsymetric_mesh.f90, which it follows): every array is
+ * a DEVICE pointer (x: imax, y: jmax, xm: imax+1, ym: jmax+1, flag / epsilon1 / liga_poros:
+ * imax x jmax column-major).  The 1-D arrays are computed on the host as acs_mesh_channel does and
+ * copied; the porous flag with its dilation sweeps and epsilon1 / liga_poros are computed by
+ * kernels on `cuda_stream` (NULL: the legacy default stream), which the call synchronises.  The
+ * results equal acs_mesh_channel's bit for bit. */
+int acs_mesh_channel_device(int imax, int jmax, double Lx, double Ly, double stretch, const double* box1,
+                            const double* box2, double porosity, double* x, double* y, double* xm, double* ym,
+                            int* flag, double* epsilon1, double* liga_poros, void* cuda_stream);
 /* Seeded uniform noise in [-amp, amp): splitmix64 of (seed, case, field, index). */
 double acs_noise(uint64_t seed, uint64_t case_id, uint64_t field, uint64_t index, double amp);
 /* out[k] = acs_noise(seed, case_id, field, index[k], amp) for k < n. */
@@ -148,6 +158,8 @@ int acs_solve_c(acs_handle* h, const double* um_n_tau, const double* vm_n_tau, c
 /* Device-resident loop state (main.f90:15-20). */
 int acs_set_field(acs_handle* h, int field, const double* host);
 int acs_get_field(acs_handle* h, int field, double* host);
+/* acs_batch_cell_fields of the handle's case */
+int acs_cell_fields(acs_handle* h, double* u, double* v, double* vel_mag);
 /* n_steps physical steps of main.f90:116-186 on the device, the whole pseudo loop in one CUDA
  * graph.  *itc is the reference's pseudo counter carried across calls (1 before the first step).
  * iters[n_steps] and err[n_steps] (may be NULL) receive each step's pseudo-iteration count and
@@ -161,6 +173,11 @@ int acs_batch_destroy(acs_batch* b);
 int acs_batch_set_stream(acs_batch* b, void* cuda_stream);
 int acs_batch_set_field(acs_batch* b, int case_id, int field, const double* host);
 int acs_batch_get_field(acs_batch* b, int case_id, int field, double* host);
+/* comp_mean (comp_mean.f90:1-25) of case case_id's physical-step velocities computed on the device:
+ * u(i,j) = (um(i+1,j) + um(i,j))/2, v(i,j) = (vm(i,j+1) + vm(i,j))/2 and sqrt(u^2 + v^2), the
+ * velocity magnitude of the ParaView output (transient.f90:69-74); host arrays imax x jmax,
+ * Fortran order.  Uses the batch's stage scratch, so call it between runs. */
+int acs_batch_cell_fields(acs_batch* b, int case_id, double* u, double* v, double* vel_mag);
 /* Runs every case for n_steps physical steps in one graph launch; converged cases drop out of
  * the launch through per-case masks.  itc[n_cases] in/out; iters/err are [n_cases*n_steps]
  * (case-major, may be NULL); status[n_cases] (may be NULL). */

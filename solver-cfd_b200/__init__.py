@@ -45,7 +45,8 @@ EXPORTED = (
     "acs_batch_run", "acs_batch_launch_count", "acs_launch_count", "acs_batch_time_kernel",
     "acs_batch_set_option", "acs_set_option", "acs_solve_u_static",
     "acs_batch_ws_enable", "acs_batch_ws_features", "acs_batch_ws_target", "acs_batch_set_start",
-    "acs_batch_set_cluster_size", "acs_batch_set_tolerance",
+    "acs_batch_set_cluster_size", "acs_batch_set_tolerance", "acs_batch_cell_fields", "acs_cell_fields",
+    "acs_mesh_channel_device",
 )
 WS_IN, WS_OUT = 11, 8
 POLICY_BEST, POLICY_PREDICTED, POLICY_PLAIN = 0, 1, 2
@@ -104,6 +105,8 @@ def _declare(L):
     L.acs_mesh_reference.argtypes = [C.c_int, C.c_double, _D, _D, _D, _D, _I, _D, _D]
     L.acs_mesh_channel.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _D, _D,
                                    C.c_double, _D, _D, _D, _D, _I, _D, _D]
+    L.acs_mesh_channel_device.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _D, _D,
+                                          C.c_double] + [C.c_void_p] * 8
     L.acs_noise.argtypes = [C.c_uint64] * 4 + [C.c_double]
     L.acs_noise.restype = C.c_double
     L.acs_noise_array.argtypes = [C.c_uint64] * 3 + [C.POINTER(C.c_uint64), C.c_longlong, C.c_double, _D]
@@ -131,6 +134,8 @@ def _declare(L):
     L.acs_set_option.argtypes = [V, C.c_int, C.c_longlong]
     L.acs_solve_u_static.argtypes = [C.POINTER(AcsParams), C.POINTER(AcsGrid), V, V, V, V, V, _D, V]
     L.acs_batch_set_cluster_size.argtypes = [V, C.c_int, C.c_int]
+    L.acs_batch_cell_fields.argtypes = [V, C.c_int, _D, _D, _D]
+    L.acs_cell_fields.argtypes = [V, _D, _D, _D]
     L.acs_batch_set_tolerance.argtypes = [V, C.c_int, C.c_double]
     L.acs_batch_ws_enable.argtypes = [V, C.c_int, C.c_int]
     L.acs_batch_ws_features.argtypes = [V, V, V]
@@ -348,6 +353,12 @@ class Case:
         _check(lib().acs_launch_count(self.h, C.byref(n)), "acs_launch_count")
         return n.value
 
+    def cell_fields(self):
+        """comp_mean on the device: cell-centred (u, v) and the velocity magnitude."""
+        out = [np.zeros((self.nx, self.ny), order="F") for _ in range(3)]
+        _check(lib().acs_cell_fields(self.h, *(_dp(a) for a in out)), "acs_cell_fields")
+        return tuple(out)
+
 
 # ---------------------------------------------------------------------------------------------
 # Batch of independent cases
@@ -417,6 +428,13 @@ class Batch:
         n = C.c_longlong(0)
         _check(lib().acs_batch_launch_count(self.h, C.byref(n)), "acs_batch_launch_count")
         return n.value
+
+    def cell_fields(self, c: int):
+        """comp_mean of case c on the device: cell-centred (u, v) and the velocity magnitude."""
+        p = self.params[c]
+        out = [np.zeros((p.imax, p.jmax), order="F") for _ in range(3)]
+        _check(lib().acs_batch_cell_fields(self.h, c, *(_dp(a) for a in out)), "acs_batch_cell_fields")
+        return tuple(out)
 
     def set_cluster_size(self, c: int, ctas: int):
         """CTAs of case c's cluster in the persistent engine (0: from OPT_NODES_PER_CTA)."""

@@ -28,6 +28,8 @@ SOURCES = {
     "kernels_exact.cu": ["-fmad=false"],
     "engine_exact.cu": ["-fmad=false"],
     "control.cu": ["-fmad=false"],
+    "output.cu": ["-fmad=false"],
+    "mesh_device.cu": [],
     "engine_fast.cu": [],
     "kernels_fast.cu": [],
     "tile_engine.cu": [],

@@ -20,6 +20,10 @@ void launch_p_fast(const CaseDev*, CaseCtl*, const Tile*, int ntiles, cudaStream
 void launch_bc_uv(const CaseDev*, const CaseCtl*, int ncases, int which, cudaStream_t);
 void launch_bc_cell(const CaseDev*, const CaseCtl*, int ncases, int which, cudaStream_t);
 
+// cell-centred u, v (comp_mean) and |U| of one case (output.cu)
+cudaError_t launch_cell_fields(const double* um, const double* vm, int nx, int ny, int pitch, double* u, double* v,
+                               double* mag, cudaStream_t s);
+
 // loop control (control.cu)
 __global__ void k_control(const CaseDev*, CaseCtl*, int* iters, double* err, int* n_active);
 __global__ void k_loop_cond(int* n_active, long long* iter_count, long long max_iters,

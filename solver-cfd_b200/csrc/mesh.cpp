@@ -102,11 +102,11 @@ int acs_mesh_reference(int imax, double porosity, double* x, double* y, double* 
   return ACS_OK;
 }
 
-int acs_mesh_channel(int imax, int jmax, double Lx, double Ly, double s, const double* box1,
-                     const double* box2, double porosity, double* x, double* y, double* xm,
-                     double* ym, int* flag_out, double* epsilon1, double* liga_poros) {
-  if (imax < 6 || jmax < 6 || !x || !y || !xm || !ym || !epsilon1 || !liga_poros) return ACS_E_ARG;
-  const int nx = imax, ny = jmax;
+}  // extern "C"
+
+// The channel mesh's 1-D arrays (x, y, xm, ym; 0-based storage of the 1-based arrays), shared by
+// acs_mesh_channel and the device generator of mesh_device.cu.
+void acs_channel_axes(int nx, int ny, double Lx, double Ly, double s, double* x, double* y, double* xm, double* ym) {
   double* X = x - 1;
   double* Y = y - 1;
   for (int i = 1; i <= nx; ++i) X[i] = Lx * ((double)(i - 1) / (double)(nx - 1));
@@ -115,6 +115,18 @@ int acs_mesh_channel(int imax, int jmax, double Lx, double Ly, double s, const d
     Y[j] = s > 0.0 ? 0.5 * Ly * (1.0 + std::tanh(s * (2.0 * xi - 1.0)) / std::tanh(s)) : Ly * xi;
   }
   staggered(nx, ny, X, Y, xm - 1, ym - 1);
+}
+
+extern "C" {
+
+int acs_mesh_channel(int imax, int jmax, double Lx, double Ly, double s, const double* box1,
+                     const double* box2, double porosity, double* x, double* y, double* xm,
+                     double* ym, int* flag_out, double* epsilon1, double* liga_poros) {
+  if (imax < 6 || jmax < 6 || !x || !y || !xm || !ym || !epsilon1 || !liga_poros) return ACS_E_ARG;
+  const int nx = imax, ny = jmax;
+  acs_channel_axes(nx, ny, Lx, Ly, s, x, y, xm, ym);
+  const double* X = x - 1;
+  const double* Y = y - 1;
   auto inside = [](const double* b, double px, double py) {
     return b && b[0] <= b[1] && px >= b[0] && px <= b[1] && py >= b[2] && py <= b[3];
   };

@@ -909,6 +909,24 @@ int acs_batch_get_field(acs_batch* h, int c, int field, double* host) {
   return acs::download_field(*h->b, c, field, host);
 }
 
+int acs_batch_cell_fields(acs_batch* h, int c, double* u, double* v, double* vel_mag) {
+  if (!h || !u || !v || !vel_mag) return acs::fail(ACS_E_ARG, "null argument");
+  Batch& b = *h->b;
+  if (c < 0 || c >= b.n) return acs::fail(ACS_E_ARG, "case id out of range");
+  const acs::CaseDev& d = b.hc[c];
+  // the results go through the T/C stage scratch of the cluster engine, which no step keeps
+  double* out[3] = {d.S2[0], d.S2[1], d.S2[2]};
+  CU(acs::launch_cell_fields(b.buf(c, 0, b.role_index(c, acs::FieldLoc{0, acs::R_PHYS})),
+                             b.buf(c, 1, b.role_index(c, acs::FieldLoc{1, acs::R_PHYS})), d.nx, d.ny, d.pitch,
+                             out[0], out[1], out[2], b.stream));
+  double* host[3] = {u, v, vel_mag};
+  for (int f = 0; f < 3; ++f)
+    CU(cudaMemcpy2DAsync(host[f], (size_t)d.nx * 8, out[f], (size_t)d.pitch * 8, (size_t)d.nx * 8, d.ny,
+                         cudaMemcpyDeviceToHost, b.stream));
+  CU(cudaStreamSynchronize(b.stream));
+  return ACS_OK;
+}
+
 int acs_batch_run(acs_batch* h, int n_steps, int* itc, int* iters, double* err, int* status) {
   if (!h) return acs::fail(ACS_E_ARG, "null handle");
   return acs::run_batch(*h->b, n_steps, itc, iters, err, status);
@@ -1171,6 +1189,12 @@ int acs_set_field(acs_handle* h, int field, const double* host) {
 int acs_get_field(acs_handle* h, int field, double* host) {
   if (!h || !host) return acs::fail(ACS_E_ARG, "null argument");
   return acs::download_field(*h->b, 0, field, host);
+}
+
+int acs_cell_fields(acs_handle* h, double* u, double* v, double* vel_mag) {
+  if (!h) return acs::fail(ACS_E_ARG, "null handle");
+  acs_batch tmp{h->b};
+  return acs_batch_cell_fields(&tmp, 0, u, v, vel_mag);
 }
 
 int acs_physical_steps(acs_handle* h, int n_steps, int* itc, int* iters, double* err, int* status) {

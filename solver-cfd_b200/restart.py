@@ -12,6 +12,8 @@ are plain text, one value (or one ``p T C`` triple) per line, written with list-
   numbers, and it is what the unmodified driver would load.
 * ``comp_mean`` is comp_mean.f90:1-25 (cell-centred u, v) and ``write_output_variables`` writes
   data/output_variables.dat as output.f90:12-18 does (x, y, u, v, p, T, C per cell, i outer).
+* ``vtk_text`` / ``write_vtk`` are the ParaView output of transient.f90:55-104;
+  ``write_case_vtk`` writes it for a device case, with comp_mean computed on the device.
 * ``restart_state`` turns restart arrays into a loop state the way ``PROGRAM main`` continues
   after ``CALL restart`` (main.f90:97-109): um_tau = um, vm_tau = vm, every other loop array 0.
 * ``save_case`` / ``load_case`` move a case's state between the device (``Case`` or one case of
@@ -96,6 +98,58 @@ def write_output_variables(path: str, x, y, um, vm, p, T, C) -> None:
         for i in range(imax):
             for j in range(jmax):
                 f.write(" ".join(_fmt(a) for a in (x[i], y[j], u[i, j], v[i, j], p[i, j], T[i, j], C[i, j])) + "\n")
+
+
+def _fortran_int(v: int, width: int) -> str:
+    """Fortran Iw: right-justified in `width` columns.  (A value wider than the field is written in
+    full; the reference's I3 / I6 would print asterisks there, which no reader accepts.)"""
+    return f"{int(v):{width}d}"
+
+
+def vtk_text(x, y, u, v, T, P, title: str = "Droplet Combustion") -> str:
+    """The ParaView file of transient.f90:55-104 as text: a STRUCTURED_GRID of the imax x jmax
+    cell nodes (x(i), y(j)), i outer and j inner, with the velocity magnitude, T and P as point
+    scalars and (u, v, 0) as vectors, every value in the reference's F14.4 format.  u, v are the
+    cell-centred velocities of comp_mean."""
+    x, y = np.asarray(x, np.float64), np.asarray(y, np.float64)
+    u, v, T, P = (np.asarray(a, np.float64) for a in (u, v, T, P))
+    imax, jmax = u.shape
+    f14 = lambda a: f"{a:14.4f}"
+    out = ["# vtk DataFile Version 3.0", title, "ASCII", "DATASET STRUCTURED_GRID",
+           "DIMENSIONS" + " " + _fortran_int(jmax, 3) + " " + _fortran_int(imax, 3) + " " + "1",
+           "POINTS" + " " + _fortran_int(jmax * imax, 6) + " " + "float"]
+    for i in range(imax):
+        for j in range(jmax):
+            out.append(f14(x[i]) + f14(y[j]) + f14(0.0))
+    out.append("POINT_DATA" + " " + _fortran_int(imax * jmax, 6))
+    out += ["SCALARS VEL_MAGNITUDE float", "LOOKUP_TABLE default"]
+    mag = np.sqrt(u * u + v * v)
+    out += [f14(mag[i, j]) for i in range(imax) for j in range(jmax)]
+    out += ["SCALARS T float", "LOOKUP_TABLE default"]
+    out += [f14(T[i, j]) for i in range(imax) for j in range(jmax)]
+    out += ["SCALARS P float", "LOOKUP_TABLE default"]
+    out += [f14(P[i, j]) for i in range(imax) for j in range(jmax)]
+    out += ["", "", "VECTORS Vectors float"]
+    out += [f14(u[i, j]) + f14(v[i, j]) + f14(0.0) for i in range(imax) for j in range(jmax)]
+    return "\n".join(out) + "\n"
+
+
+def write_vtk(path: str, x, y, u, v, T, P, title: str = "Droplet Combustion") -> None:
+    """Write `vtk_text` to `path` (the reference names it data/paraview_output<n>.vtk)."""
+    with open(path, "w") as f:
+        f.write(vtk_text(x, y, u, v, T, P, title))
+
+
+def write_case_vtk(path: str, solver, mesh: dict, case: int = 0, title: str = "Droplet Combustion") -> None:
+    """The ParaView file of a device case (a ``Case``, or case `case` of a ``Batch``): u, v and
+    the velocity magnitude from comp_mean computed on the device, T and P downloaded."""
+    if hasattr(solver, "cell_fields") and hasattr(solver, "physical_steps"):
+        u, v, _ = solver.cell_fields()
+        st = solver.get_state(("T", "p"))
+    else:
+        u, v, _ = solver.cell_fields(case)
+        st = solver.get_state(case, ("T", "p"))
+    write_vtk(path, mesh["x"], mesh["y"], u, v, st["T"], st["p"], title)
 
 
 def restart_state(arrays: dict) -> dict:

@@ -53,9 +53,12 @@ def main(ref_root):
     PTC = read_numbers(os.path.join(dc, "restart", "restartPTC.dat")).reshape(nx, ny, 3)
     gu = read_numbers(os.path.join(dc, "grid_u.dat")).reshape(nx + 1, ny, 2)
     gv = read_numbers(os.path.join(dc, "grid_v.dat")).reshape(nx, ny + 1, 2)
+    # the ParaView file the same run wrote at its end (transient.f90:55-104), kept as text
+    with open(os.path.join(dc, "paraview_output100.vtk")) as f:
+        vtk10 = f.read()
     np.savez_compressed(
         os.path.join(here, "doconcurrent_10x16.npz"),
-        imax=nx, jmax=ny, output_variables=out10,
+        imax=nx, jmax=ny, output_variables=out10, paraview_vtk=np.array(vtk10),
         um=U, vm=V, p=PTC[:, :, 0], T=PTC[:, :, 1], C=PTC[:, :, 2],
         xm=gu[:, 0, 0], y=gu[0, :, 1], x=gv[:, 0, 0], ym=gv[0, :, 1])
     print("wrote fixtures to", here)

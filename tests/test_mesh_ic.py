@@ -99,3 +99,33 @@ def test_oracle_generators_build_identical_cases(pkg, orc):
             assert np.array_equal(np.asarray(m1[k]), np.asarray(m2[k])), k
         for k in s1:
             assert np.array_equal(s1[k], s2[k]), k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("geom", [(37, 26, 1.5, 1), (153, 153, 1.5, 1), (64, 31, 0.0, 2), (20, 45, 1.5, 0)])
+def test_device_channel_mesh_equals_host(gpu, geom):
+    """acs_mesh_channel_device (porous flag, its dilation sweeps, epsilon1 and liga on the device)
+    equals acs_mesh_channel bit for bit: one box, two boxes, none, stretched and uniform y."""
+    import ctypes as C
+    import torch
+    pkg = gpu
+    nx, ny, s, nbox = geom
+    cfg = pkg.configs
+    boxes = [cfg.centred_block(2.0, 1.0, 0.3), (0.1, 0.6, 0.2, 0.55)][:nbox] if nbox else []
+    host = pkg.mesh_channel(nx, ny, 2.0, 1.0, s, boxes[0] if nbox > 0 else None, 0.45,
+                            boxes[1] if nbox > 1 else None)
+    dev = {k: torch.zeros(n, dtype=torch.float64, device="cuda")
+           for k, n in (("x", nx), ("y", ny), ("xm", nx + 1), ("ym", ny + 1), ("eps", nx * ny), ("liga", nx * ny))}
+    flag = torch.zeros(nx * ny, dtype=torch.int32, device="cuda")
+    b = [np.array(bx, float) for bx in boxes] + [None] * (2 - len(boxes))
+    ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+    code = pkg.lib().acs_mesh_channel_device(nx, ny, 2.0, 1.0, s, ptr(b[0]), ptr(b[1]), 0.45,
+                                             *(dev[k].data_ptr() for k in ("x", "y", "xm", "ym")),
+                                             flag.data_ptr(), dev["eps"].data_ptr(), dev["liga"].data_ptr(), None)
+    assert code == 0, pkg.lib().acs_last_error()
+    for k in ("x", "y", "xm", "ym"):
+        assert np.array_equal(dev[k].cpu().numpy(), host[k]), k
+    assert np.array_equal(flag.cpu().numpy().reshape((nx, ny), order="F"), host["flag"])
+    for k in ("eps", "liga"):
+        assert np.array_equal(dev[k].cpu().numpy().reshape((nx, ny), order="F"), host[k]), k
+    assert (host["flag"] == 3).any() == (nbox > 0)

@@ -56,8 +56,8 @@ def test_replicas_and_max_over_ranks(tmp_path):
     res = [np.load(tmp_path / f"rank{r}.npz") for r in range(world)]
     for r in res:
         assert float(r["max"]) == 1.5            # the slowest rank's time
-        assert int(r["n"]) == 16 and str(r["kind"]) == "full"
-    tables = res[0]["tables"].reshape(world, 16, 5)
+        assert int(r["n"]) == 64 and str(r["kind"]) == "full"
+    tables = res[0]["tables"].reshape(world, 64, 5)
     assert np.array_equal(res[0]["tables"], res[1]["tables"])   # both ranks agree on the plan
     # same case sizes on every rank (weak scaling), different cases (parameters differ)
     assert np.array_equal(tables[0][:, :2], tables[1][:, :2])

@@ -94,3 +94,36 @@ def test_checkpoint_resume_through_restart_files(gpu, orc, rs, tmp_path):
     a, b = out["vm"].copy(), ost["vm"].copy()
     a[-1, -1] = b[-1, -1] = 0.0   # vm(imax, jmax+1) is never read by the loop
     assert np.array_equal(a, b)
+
+
+def test_vtk_writer_reproduces_the_reference_file(pkg):
+    """transient.f90:55-104 writes data/paraview_output<n>.vtk; the writer, given the final
+    arrays of the reference's 10 x 16 run (its restart files) and the cell-centred velocities of
+    comp_mean, reproduces the ParaView file that run shipped, character for character."""
+    from importlib import import_module
+    r = import_module(pkg.__name__ + ".restart")
+    z = np.load(os.path.join(GOLDEN, "doconcurrent_10x16.npz"))
+    u, v = r.comp_mean(z["um"], z["vm"])
+    assert r.vtk_text(z["x"], z["y"], u, v, z["T"], z["p"]) == str(z["paraview_vtk"])
+
+
+@pytest.mark.gpu
+def test_cell_fields_on_device_equal_comp_mean(gpu):
+    """acs_batch_cell_fields: comp_mean and the velocity magnitude on the device, bit for bit the
+    host's (the reference's expression order, no fused multiply-add)."""
+    from importlib import import_module
+    r = import_module(gpu.__name__ + ".restart")
+    cfg = gpu.configs
+    items = [cfg.channel_case(37, 26, seed=3, scalars=True), cfg.reference_case(14)[:4]]
+    b = gpu.Batch([x[0] for x in items], [x[1] for x in items])
+    rng = np.random.default_rng(5)
+    for c, (prm, mesh, st, itc) in enumerate(items):
+        st = dict(st)
+        st["um"] = np.asfortranarray(rng.uniform(-1, 1, st["um"].shape))
+        st["vm"] = np.asfortranarray(rng.uniform(-1, 1, st["vm"].shape))
+        b.set_state(c, st)
+        u, v, mag = b.cell_fields(c)
+        uh, vh = r.comp_mean(st["um"], st["vm"])
+        assert np.array_equal(u, uh) and np.array_equal(v, vh)
+        assert np.array_equal(mag, np.sqrt(uh * uh + vh * vh))
+    b.close()
