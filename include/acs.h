@@ -82,7 +82,8 @@ typedef struct acs_params {
                           i.e. the velocity divergence (used by the channel configurations) */
 } acs_params;
 
-/* Grid and porous fields (module comum: x, y, xm, ym, epsilon1, liga_poros). */
+/* Grid and porous fields (module comum: x, y, xm, ym, epsilon1, liga_poros).  Host or device
+ * pointers: acs_create / acs_batch_create copy the arrays they are given. */
 typedef struct acs_grid {
   int imax, jmax;
   const double *x, *y, *xm, *ym;      /* [imax], [jmax], [imax+1], [jmax+1] */
@@ -121,7 +122,7 @@ int acs_mesh_channel(int imax, int jmax, double Lx, double Ly, double s, const d
  * imax x jmax column-major).  The 1-D arrays are computed on the host as acs_mesh_channel does and
  * copied; the porous flag with its dilation sweeps and epsilon1 / liga_poros are computed by
  * kernels on `cuda_stream` (NULL: the legacy default stream), which the call synchronises.  The
- * results equal acs_mesh_channel's bit for bit. */
+ * results equal acs_mesh_channel's bit for bit; an acs_grid may point at them directly. */
 int acs_mesh_channel_device(int imax, int jmax, double Lx, double Ly, double stretch, const double* box1,
                             const double* box2, double porosity, double* x, double* y, double* xm, double* ym,
                             int* flag, double* epsilon1, double* liga_poros, void* cuda_stream);

@@ -332,14 +332,43 @@ void reset_roles(CaseCtl& k) {
   k.tau_dirty = 1;
 }
 
-int create_batch(const acs_grid* grids, const acs_params* params, int n, Batch** out) {
-  if (!grids || !params || n <= 0 || !out) return fail(ACS_E_ARG, "null argument or n <= 0");
+// Grid arrays may be host or device pointers (acs_mesh_channel_device writes device arrays): a
+// grid with any array in device memory is copied to host storage before the pool is built.
+int host_grids(const acs_grid* grids, int n, std::vector<acs_grid>& hg, std::vector<std::vector<double>>& store) {
+  hg.assign(grids, grids + n);
+  for (int c = 0; c < n; ++c) {
+    acs_grid& g = hg[c];
+    const double** arr[6] = {&g.x, &g.y, &g.xm, &g.ym, &g.epsilon1, &g.liga_poros};
+    const size_t len[6] = {(size_t)g.imax, (size_t)g.jmax, (size_t)g.imax + 1, (size_t)g.jmax + 1,
+                           (size_t)g.imax * g.jmax, (size_t)g.imax * g.jmax};
+    for (int k = 0; k < 6; ++k) {
+      cudaPointerAttributes a{};
+      if (cudaPointerGetAttributes(&a, *arr[k]) != cudaSuccess) {
+        cudaGetLastError();
+        continue;  // not known to CUDA: host memory
+      }
+      if (a.type != cudaMemoryTypeDevice) continue;
+      store.emplace_back(len[k]);
+      if (cudaMemcpy(store.back().data(), *arr[k], sizeof(double) * len[k], cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(ACS_E_CUDA, "copying a device grid array");
+      *arr[k] = store.back().data();
+    }
+  }
+  return ACS_OK;
+}
+
+int create_batch(const acs_grid* grids_in, const acs_params* params, int n, Batch** out) {
+  if (!grids_in || !params || n <= 0 || !out) return fail(ACS_E_ARG, "null argument or n <= 0");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(ACS_E_CUDA, "no CUDA device");
   for (int c = 0; c < n; ++c) {
-    int r = validate(grids[c], params[c]);
+    int r = validate(grids_in[c], params[c]);
     if (r) return r;
   }
+  std::vector<acs_grid> hg;
+  std::vector<std::vector<double>> grid_store;
+  if (int r = host_grids(grids_in, n, hg, grid_store)) return r;
+  const acs_grid* grids = hg.data();
   const bool fast = params[0].arith == ACS_ARITH_FAST;
   for (int c = 1; c < n; ++c)
     if ((params[c].arith == ACS_ARITH_FAST) != fast) return fail(ACS_E_ARG, "all cases of a batch must use one arith mode");

@@ -129,3 +129,44 @@ def test_device_channel_mesh_equals_host(gpu, geom):
     for k in ("eps", "liga"):
         assert np.array_equal(dev[k].cpu().numpy().reshape((nx, ny), order="F"), host[k]), k
     assert (host["flag"] == 3).any() == (nbox > 0)
+
+
+@pytest.mark.gpu
+def test_case_created_from_device_grid_runs_like_host_grid(gpu):
+    """acs_create given a grid whose arrays are the device arrays of acs_mesh_channel_device runs
+    the same two physical steps as the case created from the host mesh, bit for bit."""
+    import ctypes as C
+    import torch
+    pkg = gpu
+    params, mesh, state, itc = pkg.configs.channel_case(40, 30, seed=5, Re=150.0, block=pkg.configs.centred_block(2.0, 1.0, 0.3),
+                                                        porosity=0.45, Da=1e-3, Cf=0.55, Ri=1.0, scalars=True)
+    nx, ny = params.imax, params.jmax
+    box = np.array(pkg.configs.centred_block(2.0, 1.0, 0.3), float)
+    dev = {k: torch.zeros(n, dtype=torch.float64, device="cuda")
+           for k, n in (("x", nx), ("y", ny), ("xm", nx + 1), ("ym", ny + 1), ("eps", nx * ny), ("liga", nx * ny))}
+    flag = torch.zeros(nx * ny, dtype=torch.int32, device="cuda")
+    L = pkg.lib()
+    code = L.acs_mesh_channel_device(nx, ny, 2.0, 1.0, 1.5, box.ctypes.data_as(C.POINTER(C.c_double)), None, 0.45,
+                                     *(dev[k].data_ptr() for k in ("x", "y", "xm", "ym")), flag.data_ptr(),
+                                     dev["eps"].data_ptr(), dev["liga"].data_ptr(), None)
+    assert code == 0, L.acs_last_error()
+    assert np.array_equal(dev["eps"].cpu().numpy().reshape((nx, ny), order="F"), mesh["eps"])
+    g = pkg.AcsGrid()
+    g.imax, g.jmax = nx, ny
+    D = C.POINTER(C.c_double)
+    g.x, g.y, g.xm, g.ym, g.epsilon1, g.liga_poros = [C.cast(C.c_void_p(dev[k].data_ptr()), D)
+                                                      for k in ("x", "y", "xm", "ym", "eps", "liga")]
+    p = params.struct()
+    h = C.c_void_p()
+    assert L.acs_create(C.byref(g), C.byref(p), C.byref(h)) == 0, L.acs_last_error()
+    a = pkg.Case.__new__(pkg.Case)
+    a.params, a.nx, a.ny, a._keep, a._p, a.h = params, nx, ny, [], p, h
+    b = pkg.Case(params, mesh)
+    out = []
+    for c in (a, b):
+        c.set_state(state)
+        out.append((c.physical_steps(2, itc)[:2], c.get_state()))
+        c.close()
+    assert np.array_equal(out[0][0][1], out[1][0][1])
+    for k in out[0][1]:
+        assert np.array_equal(out[0][1][k], out[1][1][k]), k

@@ -231,12 +231,15 @@ def test_warm_start_ablation(gpu, ws_mod, capsys):
         print("\nwarm start ablation, pseudo-iterations over steps 3..13 of 2 held-out 24x24 cases:", tot,
               "training losses", [round(x, 4) for x in losses[::50]],
               "starts plain/extrap/learned", kept, "final-field error vs plain", err)
-    # the method without the network is the plain start
+    # Against the reference's (plain) start the warm start saves more than half the work.
     assert tot["learned"] < tot["plain"] / 2.0, tot
-    # the trained network's start has the smallest initial residual on most steps.  Whether that
-    # also saves pseudo-iterations against the extrapolated start varies between training runs
-    # (the split-K gradient sums are not ordered): the count depends on smooth start errors that
-    # the max-norm residual barely sees.  Printed above, not asserted.
+    # The method without the network is the extrapolated start (the network's head starts at zero,
+    # so an untrained network gives exactly that start).  Negative result: the trained network
+    # does not reliably beat it.  Its start has the smallest initial residual on most steps, but
+    # the pseudo-iteration count over these steps was below the extrapolated start's in 2 of 7
+    # training runs (26,019 and 72,275 against 72,625) and above it in 5 (73,162 to 119,959): the
+    # count depends on smooth start errors that the max-norm residual barely sees, and training is
+    # not bit-reproducible (the split-K gradient sums are not ordered).  Printed above, not asserted.
     assert kept[2] >= 0.5, kept
     # the loop iterates to the same tolerance from either start: velocities and scalars agree with
     # the plain run to 1e-4; the pressure, which converges slowest in pseudo time, to 1e-2 (observed
@@ -244,3 +247,47 @@ def test_warm_start_ablation(gpu, ws_mod, capsys):
     for e in err:
         assert max(e["um"], e["vm"], e["T"], e["C"]) < 1e-4, e
         assert e["pn"] < 1e-2, e
+
+
+def test_final_fields_against_tightly_converged_run(gpu, ws_mod, capsys):
+    """How far runs at residual 1e-6 end from the converged solution: the plain and the
+    extrapolated-start runs of two 24 x 24 cases, 10 physical steps each, against the same cases
+    iterated to residual 1e-10 with the plain start, and the extrapolated start again with its
+    warm-started steps iterated to 1e-7 (the warm-tolerance policy)."""
+    pkg = gpu
+    from dataclasses import replace
+    cases = [_case(pkg, seed=3, case_id=k, Re=[280.0, 240.0][k], Ri=[1.4, 0.7][k], itc_max=2000000)
+             for k in range(2)]
+    H = W = 32
+    steps = 10
+
+    def run(eps, mode, warm_eps=None):
+        b = _batch(pkg, [(replace(c[0], eps=eps),) + tuple(c[1:]) for c in cases])
+        w = ws_mod.WarmStart(b, H, W)
+        itc = np.ones(2, np.int32)
+        total = 0
+        for _ in range(steps):
+            itc, it, _, _ = w.step(itc, mode, warm_eps=warm_eps)
+            total += int(it.sum())
+        out = [b.get_state(c, ("um", "vm", "pn", "T", "C")) for c in range(2)]
+        b.close()
+        return out, total
+
+    ref, n_ref = run(1e-10, "plain")
+    runs = {"plain 1e-6": run(1e-6, "plain"), "extrap 1e-6": run(1e-6, "extrap"),
+            "extrap 1e-7": run(1e-6, "extrap", warm_eps=1e-7)}
+    err = {name: {k: max(ws_mod.field_error(o[c], ref[c])[k] for c in range(2)) for k in ("um", "vm", "pn", "T", "C")}
+           for name, (o, _) in runs.items()}
+    with capsys.disabled():
+        print(f"\nfinal fields after {steps} steps against the run converged to 1e-10 ({n_ref} pseudo-iterations),"
+              " relative max-norm difference:")
+        for name, e in err.items():
+            print(f"   {name} ({runs[name][1]} pseudo-iterations)", {k: f"{v:.2e}" for k, v in e.items()})
+    worst = {name: max(e.values()) for name, e in err.items()}
+    # every run at 1e-6 ends close to the converged solution; the extrapolated start's error is of
+    # the order of the plain run's own, and a tighter tolerance on its warm-started steps reduces it
+    for name, w in worst.items():
+        assert w < 1e-2, (name, err[name])
+    assert worst["extrap 1e-6"] < 10.0 * worst["plain 1e-6"], err
+    assert worst["extrap 1e-7"] < worst["extrap 1e-6"], err
+    assert runs["extrap 1e-6"][1] < runs["plain 1e-6"][1], {k: v[1] for k, v in runs.items()}
