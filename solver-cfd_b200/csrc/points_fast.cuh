@@ -130,6 +130,14 @@ struct PtFastT {
   static __device__ __forceinline__ double rv_at(const CaseDev& d, const double* um, const double* vm,
                                                  const double* p, double T0, double T1, int P, long long q,
                                                  bool por, int i, int j) {
+    const double w = (d.flags & F_BUOY) ? 1.0 - 2.0 / (T0 + T1) : 0.0;
+    return rv_at_w(d, um, vm, p, w, P, q, por, i, j);
+  }
+  // Same, with the buoyancy factor w = 1 - 2/(T(i,j) + T(i,j-1)) given (read only with buoyancy):
+  // T is the physical-step temperature, so w changes only between physical steps.
+  static __device__ __forceinline__ double rv_at_w(const CaseDev& d, const double* um, const double* vm,
+                                                   const double* p, double w, int P, long long q, bool por, int i,
+                                                   int j) {
     const double e = por ? d.phi : 1.0, ie = por ? d.fc[FC_IPHI] : 1.0;
     const Met X = MX(d, i), Xe = MX(d, i + 1), Y = MY(d, j), Ys = MY(d, j - 1);
     const double vP = F(vm, q), vW = F(vm, q - 1), vE = F(vm, q + 1), vS = F(vm, q - P), vN = F(vm, q + P);
@@ -155,7 +163,7 @@ struct PtFastT {
       const double dydudx = X.dm * (F(um, q + 1) - F(um, q)) * X.rdm - X.dm * (F(um, q + 1 - P) - F(um, q - P)) * X.rdm;
       r += d.b_art * (dydudx + dvdydy);
     }
-    if (d.flags & F_BUOY) r += d.InvFr2 * (1.0 - 2.0 / (T0 + T1));
+    if (d.flags & F_BUOY) r += d.InvFr2 * w;
     if (por) {
       const double uP = F(um, q);
       r -= e * vP * (d.fc[FC_IREDA] + d.fc[FC_CFS] * sqrt(fma(uP, uP, vP * vP)));

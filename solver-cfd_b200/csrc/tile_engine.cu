@@ -89,6 +89,7 @@ int te_encode_maps(const std::vector<CaseDev>& cases, TeMaps* maps) {
     for (int b = 0; b < 3; ++b) ok = ok && make(&maps[c].t33[b], d.T[b], TE_TILE, TE_TILE + 1);
     ok = ok && make(&maps[c].liga32, d.liga, TE_TILE, TE_TILE);
     ok = ok && make(&maps[c].liga36, d.liga, TE_BOX_UV, TE_BOX_UV);
+    ok = ok && make(&maps[c].buoyw, d.S2[3], TE_TILE, TE_TILE);
     if (!ok) return 2;
   }
   return 0;
@@ -339,6 +340,9 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
   const int rv_tau = kc->rv[R_TAU], rv_phys = kc->rv[R_PHYS], rv_ntau = kc->rv[R_NTAU];
   const int rt_phys = kc->rt[R_PHYS], rp_read = kc->rp_read;
   const bool buoy = (cs[t.c].flags & F_BUOY) != 0;
+  // the buoyancy factor w = 1 - 2/(T(i,j) + T(i,j-1)) of the physical-step temperature: stage 1 of
+  // a step's first pseudo-iteration computes it from T and stores it, every other launch loads it
+  const bool fresh = ST == 1 && kc->k == 0;
 
   double* Ub = reinterpret_cast<double*>(sm);  // um_tau box
   double* Vb = Ub + BU * BU;                   // vm_tau box
@@ -349,7 +353,7 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
                                                          // after the vm_tau copy for V)
   double* Vm = Um + NT * NT;                   // vm, then the V stage output
   double* Lg = Vm + NT * NT;                   // liga
-  double* Tb = Lg + NT * NT;                   // T, rows j0-1 .. j0+31
+  double* Tb = Lg + NT * NT;                   // T, rows j0-1 .. j0+31 (or w, rows j0 .. j0+31)
   double* Ms = Tb + NT * (NT + 1);             // metric slices
   double* Mt = Ms + 4 * MS_UV;
 
@@ -358,7 +362,8 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
   if (threadIdx.x == 0) mbar_init(&bar);
   __syncthreads();
   if (threadIdx.x == 0) {
-    mbar_expect(&bar, (ST == 1 ? 3u : 5u) * BOX_UV_BYTES + 3u * NT * NT * 8 + (buoy ? NT * (NT + 1) * 8u : 0u));
+    mbar_expect(&bar, (ST == 1 ? 3u : 5u) * BOX_UV_BYTES + 3u * NT * NT * 8 +
+                          (buoy ? (fresh ? NT * (NT + 1) * 8u : NT * NT * 8u) : 0u));
     tma_load(Ub, &M->uv[TE_U + ru_tau], x0 - 2, y0 - 2, &bar);
     tma_load(Vb, &M->uv[TE_V + rv_tau], x0 - 2, y0 - 2, &bar);
     tma_load(Pb, &M->uv[TE_P + rp_read], x0 - 2, y0 - 2, &bar);
@@ -369,7 +374,8 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
     tma_load(Um, &M->pt[TE_U + ru_phys], x0, y0, &bar);
     tma_load(Vm, &M->pt[TE_V + rv_phys], x0, y0, &bar);
     tma_load(Lg, &M->liga32, x0, y0, &bar);
-    if (buoy) tma_load(Tb, &M->t33[rt_phys], x0, y0 - 1, &bar);
+    if (buoy && fresh) tma_load(Tb, &M->t33[rt_phys], x0, y0 - 1, &bar);
+    if (buoy && !fresh) tma_load(Tb, &M->buoyw, x0, y0, &bar);
   }
   load_case(&d, cs + t.c);
   const CaseDev& dg = cs[t.c];
@@ -412,8 +418,16 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
     // both residuals for every node of the tile (the boxes hold every neighbour), kept only at
     // interior nodes: no branch separates the two chains
     const double RU = PS::ru_at(d, Ui, Vb, Pb, BU, qs, por, i, j);
-    const double T0 = buoy ? Tb[li + (lj + 1) * NT] : 1.0, T1 = buoy ? Tb[li + lj * NT] : 1.0;
-    const double RV = PS::rv_at(d, Ub, Vs, Pb, T0, T1, BU, qs, por, i, j);
+    double w = 0.0;
+    if (buoy) {
+      if (fresh) {
+        w = 1.0 - 2.0 / (Tb[li + (lj + 1) * NT] + Tb[li + lj * NT]);
+        if (i <= nx && j <= ny + 1) d.S2[3][lin(i, j, d.pitch)] = w;  // v nodes only: inside the buffer
+      } else {
+        w = Tb[li + lj * NT];
+      }
+    }
+    const double RV = PS::rv_at_w(d, Ub, Vs, Pb, w, BU, qs, por, i, j);
     const double ut = Ub[qs], vt = Vb[qs];
     const double ru = ((Um[qo] - ut) + RU * d.dt) * d.dtau;
     const double rv = ((Vm[qo] - vt) + RV * d.dt) * d.dtau;

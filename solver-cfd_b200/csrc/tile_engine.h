@@ -30,6 +30,7 @@ struct TeMaps {
   CUtensorMap pt[TE_NBUF];   // 32 x 32 boxes (pointwise inputs: um, vm, p)
   CUtensorMap t33[3];        // 32 x 33 boxes of T[0..2] (buoyancy reads T(i,j) and T(i,j-1))
   CUtensorMap liga32, liga36;  // the porosity indicator liga (1 in the porous block, else 0)
+  CUtensorMap buoyw;         // 32 x 32 boxes of the buoyancy factor (CaseDev::S2[3])
 };
 
 // Tile origins of one case, 1-based node (i0, j0): x = i-1 in [0, pitch), y = j-1 in [0, ny+1)
