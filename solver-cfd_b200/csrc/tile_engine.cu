@@ -480,61 +480,88 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
 }
 
 // ---- P, then T and C (three stages each) -------------------------------------------------------
-// Shared memory (doubles): un, vn, T_tau, C_tau boxes (40 x 40, the tile plus four nodes); T, C
-// and liga (36 x 36, the tile plus two); p (32 x 32, overwritten in place by pn); two stage buffers
-// (36 x 36); the metric slices.  Stage s of T / C covers the tile grown by g = 3 - s nodes, i.e.
-// positions [2-g, 34+g) of the 36 x 36 layout.
+// Shared memory (doubles): un, vn, T_tau, C_tau boxes (40 x 40, the tile plus four nodes); liga
+// (36 x 36, the tile plus two); two stage buffers per scalar (36 x 36); p (32 x 32, overwritten in
+// place by pn); the metric slices.  The physical-step T and C, read once per node and stage, come
+// through the read-only cache.  Stage s of T and C covers the tile grown by g = 3 - s nodes, i.e.
+// positions [2-g, 34+g) of the 36 x 36 layout; one pass computes both scalars at each node, so the
+// two share their loads of un, vn, liga and the metrics, and the stages of T and C share barriers.
 constexpr int MS_PTC = 38;  // metric entries i0-2 .. i0+35
 constexpr size_t SMEM_PTC2 = 4 * (size_t)BOX_PTC_BYTES + 5 * (size_t)BOX_UV_BYTES + NT * NT * 8 + 2 * MS_PTC * 32;
 
-// stage ST (1..3) of one scalar (T: IS_C = false, C: IS_C = true) on the tile grown by 3 - ST
-// nodes, then bcZ / bcC there (only where the region holds boundary cells: `edge`)
-template <bool IS_C, int ST>
-__device__ __forceinline__ void scalar_stage(const CaseDev& d, const Tile& t, const double* Un, const double* Vn,
-                                             const double* Z, const double* Zp, const double* Lg, double* S1,
-                                             double* S2, double zin, bool edge) {
+struct ScalarSet {
+  const double* Z;    // the tau box (40 x 40)
+  const double* Zp;   // the physical-step array (global, pitched)
+  double* S1;         // stage buffers (36 x 36)
+  double* S2;
+  double zin;         // inflow value
+};
+
+// stage ST (1..3) of T and of C on the tile grown by 3 - ST nodes, then bcZ and bcC there (only
+// where the region holds boundary cells: `edge`)
+template <int ST>
+__device__ __forceinline__ void scalar_stage2(const CaseDev& d, const Tile& t, const double* Un, const double* Vn,
+                                              const double* Lg, const ScalarSet& T, const ScalarSet& C, bool edge) {
   using PS = PtFastT<LdShared<MS_PTC>>;
   constexpr int g = 3 - ST, e = NT + 2 * g, o36 = 2 - g, o40 = 4 - g;
   constexpr int Pz = ST == 1 ? BP : BU;
-  const double* zin_s = ST == 1 ? Z : ST == 2 ? S1 : S2;
-  double* zout = ST == 2 ? S2 : S1;
+  const double* tin = ST == 1 ? T.Z : ST == 2 ? T.S1 : T.S2;
+  const double* cin = ST == 1 ? C.Z : ST == 2 ? C.S1 : C.S2;
+  double* tout = ST == 2 ? T.S2 : T.S1;
+  double* cout = ST == 2 ? C.S2 : C.S1;
   const int nx = d.nx, ny = d.ny;
   for (int q = threadIdx.x; q < e * e; q += blockDim.x) {
     const int a = q % e, b = q / e;
     const int i = t.i0 - g + a, j = t.j0 - g + b;
     if (i >= 2 && i <= nx - 1 && j >= 2 && j <= ny - 1) {
       const int q36 = (o36 + a) + (o36 + b) * BU, q40 = (o40 + a) + (o40 + b) * BP;
-      const double Rz = PS::template rs_at<IS_C>(d, Un, Vn, BP, q40, zin_s, Pz, ST == 1 ? q40 : q36,
-                                                 Lg[q36] != 0.0, i, j);
-      const double zt = Z[q40];
-      const double rr = ((Zp[q36] - zt) + Rz * d.dt) * d.dtau;
-      if (ST == 1) zout[q36] = zt + rr;
-      else if (ST == 2) zout[q36] = 0.75 * zt + 0.25 * (S1[q36] + rr);
-      else zout[q36] = 1.0 / 3.0 * zt + 2.0 / 3.0 * (S2[q36] + rr);
+      const int qz = ST == 1 ? q40 : q36;
+      const bool por = Lg[q36] != 0.0;
+      const long long qg = lin(i, j, d.pitch);
+      const double Rt = PS::template rs_at<false>(d, Un, Vn, BP, q40, tin, Pz, qz, por, i, j);
+      const double Rc = PS::template rs_at<true>(d, Un, Vn, BP, q40, cin, Pz, qz, por, i, j);
+      const double tt = T.Z[q40], ct = C.Z[q40];
+      const double rt = ((__ldg(T.Zp + qg) - tt) + Rt * d.dt) * d.dtau;
+      const double rc = ((__ldg(C.Zp + qg) - ct) + Rc * d.dt) * d.dtau;
+      if (ST == 1) {
+        tout[q36] = tt + rt;
+        cout[q36] = ct + rc;
+      } else if (ST == 2) {
+        tout[q36] = 0.75 * tt + 0.25 * (T.S1[q36] + rt);
+        cout[q36] = 0.75 * ct + 0.25 * (C.S1[q36] + rc);
+      } else {
+        tout[q36] = 1.0 / 3.0 * tt + 2.0 / 3.0 * (T.S2[q36] + rt);
+        cout[q36] = 1.0 / 3.0 * ct + 2.0 / 3.0 * (C.S2[q36] + rc);
+      }
     }
   }
   __syncthreads();
   if (edge) {
-    const Win w{zout + o36 + o36 * BU, t.i0 - g, t.j0 - g, e, e, BU};
-    bc_cell_pass(d, w, 0, false, zin);
+    const Win wt{tout + o36 + o36 * BU, t.i0 - g, t.j0 - g, e, e, BU};
+    const Win wc{cout + o36 + o36 * BU, t.i0 - g, t.j0 - g, e, e, BU};
+    bc_cell_pass(d, wt, 0, false, T.zin);
+    bc_cell_pass(d, wc, 0, false, C.zin);
     __syncthreads();
-    bc_cell_pass(d, w, 1, false, zin);
+    bc_cell_pass(d, wt, 1, false, T.zin);
+    bc_cell_pass(d, wc, 1, false, C.zin);
     __syncthreads();
   }
 }
 
-template <bool IS_C>
-__device__ void te_scalar(const CaseDev& d, const Tile& t, const double* Un, const double* Vn, const double* Z,
-                          const double* Zp, const double* Lg, double* S1, double* S2, double* zo_g, double zin,
-                          bool edge) {
-  scalar_stage<IS_C, 1>(d, t, Un, Vn, Z, Zp, Lg, S1, S2, zin, edge);
-  scalar_stage<IS_C, 2>(d, t, Un, Vn, Z, Zp, Lg, S1, S2, zin, edge);
-  scalar_stage<IS_C, 3>(d, t, Un, Vn, Z, Zp, Lg, S1, S2, zin, edge);
+__device__ void te_scalars(const CaseDev& d, const Tile& t, const double* Un, const double* Vn, const double* Lg,
+                           const ScalarSet& T, const ScalarSet& C, double* to_g, double* co_g, bool edge) {
+  scalar_stage2<1>(d, t, Un, Vn, Lg, T, C, edge);
+  scalar_stage2<2>(d, t, Un, Vn, Lg, T, C, edge);
+  scalar_stage2<3>(d, t, Un, Vn, Lg, T, C, edge);
   const int nx = d.nx, ny = d.ny;
   for (int q = threadIdx.x; q < NT * NT; q += blockDim.x) {
     const int a = q % NT, b = q / NT;
     const int i = t.i0 + a, j = t.j0 + b;
-    if (i <= nx && j <= ny) zo_g[lin(i, j, d.pitch)] = S1[(2 + a) + (2 + b) * BU];
+    if (i <= nx && j <= ny) {
+      const int q36 = (2 + a) + (2 + b) * BU;
+      to_g[lin(i, j, d.pitch)] = T.S1[q36];
+      co_g[lin(i, j, d.pitch)] = C.S1[q36];
+    }
   }
 }
 
@@ -558,12 +585,12 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_ptc(const CaseDev* __restr
   double* Vn = Un + BP * BP;
   double* Zt = Vn + BP * BP;  // T_tau
   double* Zc = Zt + BP * BP;  // C_tau
-  double* Tp = Zc + BP * BP;  // T
-  double* Cp = Tp + BU * BU;  // C
-  double* Lg = Cp + BU * BU;  // liga
-  double* S1 = Lg + BU * BU;
-  double* S2 = S1 + BU * BU;
-  double* P0 = S2 + BU * BU;  // p, then pn
+  double* Lg = Zc + BP * BP;  // liga
+  double* S1t = Lg + BU * BU;  // stage buffers of T and C
+  double* S2t = S1t + BU * BU;
+  double* S1c = S2t + BU * BU;
+  double* S2c = S1c + BU * BU;
+  double* P0 = S2c + BU * BU;  // p, then pn
   double* Ms = P0 + NT * NT;
   double* Mt = Ms + 4 * MS_PTC;
   const TeMaps* M = maps + t.c;
@@ -571,15 +598,13 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_ptc(const CaseDev* __restr
   if (threadIdx.x == 0) mbar_init(&bar);
   __syncthreads();
   if (threadIdx.x == 0) {
-    mbar_expect(&bar, 2u * BOX_PTC_BYTES + NT * NT * 8u + (scal ? 2u * BOX_PTC_BYTES + 3u * BOX_UV_BYTES : 0u));
+    mbar_expect(&bar, 2u * BOX_PTC_BYTES + NT * NT * 8u + (scal ? 2u * BOX_PTC_BYTES + BOX_UV_BYTES : 0u));
     tma_load(Un, &M->ptc[TE_U + ru_ntau], x0 - 4, y0 - 4, &bar);
     tma_load(Vn, &M->ptc[TE_V + rv_ntau], x0 - 4, y0 - 4, &bar);
     tma_load(P0, &M->pt[TE_P + rp0], x0, y0, &bar);
     if (scal) {
       tma_load(Zt, &M->ptc[TE_T + rt_tau], x0 - 4, y0 - 4, &bar);
       tma_load(Zc, &M->ptc[TE_C + rc_tau], x0 - 4, y0 - 4, &bar);
-      tma_load(Tp, &M->uv[TE_T + rt_phys], x0 - 2, y0 - 2, &bar);
-      tma_load(Cp, &M->uv[TE_C + rc_phys], x0 - 2, y0 - 2, &bar);
       tma_load(Lg, &M->liga36, x0 - 2, y0 - 2, &bar);
     }
   }
@@ -629,9 +654,8 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_ptc(const CaseDev* __restr
     }
   }
   if (!scal) return;
-  te_scalar<false>(d, t, Un, Vn, Zt, Tp, Lg, S1, S2, d.T[rt_ntau], d.T_in, edge);
-  __syncthreads();
-  te_scalar<true>(d, t, Un, Vn, Zc, Cp, Lg, S1, S2, d.C[rc_ntau], d.C_in, edge);
+  const ScalarSet T{Zt, d.T[rt_phys], S1t, S2t, d.T_in}, C{Zc, d.C[rc_phys], S1c, S2c, d.C_in};
+  te_scalars(d, t, Un, Vn, Lg, T, C, d.T[rt_ntau], d.C[rc_ntau], edge);
 }
 
 }  // namespace
