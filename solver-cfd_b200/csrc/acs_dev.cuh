@@ -114,4 +114,35 @@ __device__ inline void block_max_to(unsigned long long* slot, double v) {
   }
 }
 
+// Block-wide max of two sets of non-negative values, one atomic each per block (one barrier).
+__device__ inline void block_max2_to(unsigned long long* slot_a, double a, unsigned long long* slot_b, double b) {
+  __shared__ double red2[2][32];
+  unsigned m = 0xffffffffu;
+  for (int o = 16; o > 0; o >>= 1) {
+    const double wa = __shfl_xor_sync(m, a, o), wb = __shfl_xor_sync(m, b, o);
+    a = (wa > a || wa != wa) ? wa : a;
+    b = (wb > b || wb != wb) ? wb : b;
+  }
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  const int nw = (blockDim.x * blockDim.y + 31) / 32;
+  if ((tid & 31) == 0) {
+    red2[0][tid >> 5] = a;
+    red2[1][tid >> 5] = b;
+  }
+  __syncthreads();
+  if (tid < 32) {
+    a = tid < nw ? red2[0][tid] : 0.0;
+    b = tid < nw ? red2[1][tid] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double wa = __shfl_xor_sync(m, a, o), wb = __shfl_xor_sync(m, b, o);
+      a = (wa > a || wa != wa) ? wa : a;
+      b = (wb > b || wb != wb) ? wb : b;
+    }
+    if (tid == 0) {
+      if (a != 0.0) atomic_max_nonneg(slot_a, a);
+      if (b != 0.0) atomic_max_nonneg(slot_b, b);
+    }
+  }
+}
+
 }  // namespace acs

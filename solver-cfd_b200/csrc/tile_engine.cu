@@ -451,11 +451,7 @@ __global__ void __launch_bounds__(TE_THREADS, 2) k_te_uv(const CaseDev* __restri
       if (ST == 3) mv = nanmax(mv, fabs(rv));
     }
   }
-  if (ST == 3) {
-    block_max_to(&ctl[t.c].res_u, mu);
-    __syncthreads();  // block_max_to's reduction slots are reused by the second call
-    block_max_to(&ctl[t.c].res_v, mv);
-  }
+  if (ST == 3) block_max2_to(&ctl[t.c].res_u, mu, &ctl[t.c].res_v, mv);
   __syncthreads();
   // boundary passes, only where the tile holds boundary nodes (u: i in {1,2,nx,nx+1} or
   // j in {1,ny}; v: i in {1,nx} or j in {1,2,ny,ny+1})
