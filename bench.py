@@ -2,25 +2,28 @@
 
 A bench step is one converged physical step (a pseudo-time loop run to max residual < eps) of
 every case of the workload; the unit is converged case-steps per second.  ``value`` is the
-whole-job throughput with the state resident in HBM; ``e2e`` is the same steps again through the
-C ABI with the state copied from pinned host buffers before and back after every step.
+whole-job throughput with the state resident in HBM; ``e2e`` is the first ``--sample-steps``
+of the same steps again through the C ABI with the state copied from pinned host buffers before
+and back after every step.
 
 The default workload, ws-153, is the learned-warm-start configuration: 64 held-out cases at
 153 x 153 drawn from the batched configuration's parameter distribution (seed 101; the network
 trained on seed 100), the tile engine, FAST arithmetic.  The W warm-up steps run from rest with
 the reference's (plain) start, recording the warm-start history; the K timed steps each start
 from the best of the plain, extrapolated and learned start (the U-Net inference and the start
-selection inside the timed region).  The plain GPU path is timed on the first steps of the same
-window from the same state (``plain_gpu``).
+selection inside the timed region).  The plain GPU path is timed on the first ``--sample-steps``
+steps of the same window from the same state (``plain_gpu``).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--engine tile|cluster|graph]
     python bench.py --impl reference ...   # the CPU implementation of the loop on host cores
 
 The reference arm runs the oracle (the C++ restatement of the reference's OpenMP loop; no
-Fortran compiler exists here) on all host cores: for a sample of the workload's cases it runs
-the W warm-up steps and then times the K steps of the same window, every step converged to the
-same tolerance with the reference's start.  Its cases are built with the oracle's own mesh and
-noise generators, so it never loads this package's library.
+Fortran compiler exists here) on all host cores: for a sample of the workload's cases
+(``--ref-cases``) it converges the W warm-up steps from rest and then times the first
+``--sample-steps`` steps of the same window (the steps the product's e2e pass replays), every step
+converged to the same tolerance with the reference's start.  A converged CPU step of a 153 x 153
+case takes one to four minutes, so the sample is bounded to those steps.  Its cases are built
+with the oracle's own mesh and noise generators, so it never loads this package's library.
 
 Multi-GPU (torchrun): each rank runs its own replica of the workload (cases are independent, so
 there is no exchange on the data path); the elapsed time is the max over ranks.
@@ -538,9 +541,10 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
     if world > 1:
         dist.barrier()
     itc = itc_snap.copy()
-    it_e2e = np.zeros((n_cases, args.steps), np.int64)
+    n_e2e = max(1, min(args.steps, args.sample_steps))
+    it_e2e = np.zeros((n_cases, n_e2e), np.int64)
     t0 = time.perf_counter()
-    for k in range(args.steps):
+    for k in range(n_e2e):
         for c in range(n_cases):
             C_.set_state(c, {nme: v for nme, (t, v) in host[c].items()})
         itc, it, _ = ws_step(wC, C_, itc)
@@ -552,7 +556,7 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
     C_.close()
 
     # ---- plain GPU path on the first m steps of the window from the same state, one launch
-    m = max(1, min(args.steps, args.plain_steps))
+    m = max(1, min(args.steps, args.plain_steps if args.plain_steps is not None else args.sample_steps))
     B = make(snap)
     if world > 1:
         dist.barrier()
@@ -655,9 +659,10 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
             "unet_inference": {"bound": "tensor", "flops_per_launch_set": fwd_flops, "ms": fwd_ms,
                                "achieved_tflops": fwd_flops / (fwd_ms * 1e-3) / 1e12,
                                "peak_tflops": bf16_peak, "frac": fwd_flops / (fwd_ms * 1e-3) / 1e12 / bf16_peak},
-            "e2e": {"value": n_cases * args.steps * world / e2e_el, "unit": "steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "steps": args.steps,
-                    "same_iterations_as_timed": bool((it_e2e == iters_ws).all())},
+            "e2e": {"value": n_cases * n_e2e * world / e2e_el, "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": n_e2e,
+                    "sample": f"the first {n_e2e} of the {args.steps} timed steps, replayed from the same state",
+                    "same_iterations_as_timed": bool((it_e2e == iters_ws[:, :n_e2e]).all())},
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
@@ -703,6 +708,7 @@ def run_reference(args):
     n = len(items)
     ns = max(1, min(args.ref_cases, n))
     picks = sorted({int(round(q * (n - 1) / max(1, ns - 1))) for q in range(ns)}) if ns > 1 else [0]
+    n_steps = max(1, min(args.steps, args.sample_steps))
     t_all = time.perf_counter()
     secs = 0.0
     iters = {}
@@ -713,11 +719,11 @@ def run_reference(args):
         if args.warmup:
             itc, _, _ = o.run(s, args.warmup, itc)
         t0 = time.perf_counter()
-        itc, it, _ = o.run(s, args.steps, itc)
+        itc, it, _ = o.run(s, n_steps, itc)
         secs += time.perf_counter() - t0
         iters[str(c)] = [int(v) for v in it]
     wall = time.perf_counter() - t_all
-    value = len(picks) * args.steps / secs
+    value = len(picks) * n_steps / secs
     line = {
         "impl": "reference",
         "metric": "converged physical steps/s at pseudo-time residual 1e-6",
@@ -726,19 +732,20 @@ def run_reference(args):
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": secs / args.steps * 1e3,
+        "ms_per_step": secs / n_steps * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded channel cases; no public dataset)",
         "config": {"workload": args.workload, "description": WORKLOADS[args.workload], "cases": n,
-                   "sampled_cases": picks, "pseudo_iterations_per_step": iters,
+                   "sampled_cases": picks, "timed_steps": f"the first {n_steps} of the {args.steps} timed steps",
+                   "pseudo_iterations_per_step": iters,
                    "start": "the reference's (plain) start in every step, warm-up included"},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
-                         "sample": f"cases {picks} of the {n}: {args.warmup} warm-up steps from rest, then "
-                                   f"{args.steps} timed converged steps each, one case at a time on all "
-                                   f"{threads} host threads"},
+                         "sample": f"cases {picks} of the {n}: {args.warmup} warm-up steps from rest, then the "
+                                   f"first {n_steps} of the {args.steps} timed steps, converged, one case at a "
+                                   f"time on all {threads} host threads"},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": wall,
     }
@@ -761,8 +768,12 @@ def main():
                     help="cluster engine: threads,ctas_per_sm,nodes_per_cta (skip the autotuner)")
     ap.add_argument("--stage", type=int, default=1, choices=[0, 1],
                     help="cluster engine: stage stencil arrays in shared memory (1) or read them from L1/L2 (0)")
-    ap.add_argument("--plain-steps", type=int, default=3,
-                    help="ws-* workloads: steps of the window on which the plain GPU path is timed")
+    ap.add_argument("--sample-steps", type=int, default=2,
+                    help="ws-* workloads: the first steps of the timed window that the e2e pass replays, the "
+                         "plain GPU path times and the reference arm converges on the CPU")
+    ap.add_argument("--plain-steps", type=int, default=None,
+                    help="ws-* workloads: steps of the window on which the plain GPU path is timed "
+                         "(default: --sample-steps)")
     ap.add_argument("--extrap-order", type=int, default=1, choices=[1, 2],
                     help="warm-start workload: linear (1) or quadratic (2) extrapolated candidate")
     ap.add_argument("--warm-eps", type=float, default=None,
@@ -770,7 +781,7 @@ def main():
                          "(default: every case keeps its own, 1e-6)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--ref-cases", type=int, default=2,
+    ap.add_argument("--ref-cases", type=int, default=1,
                     help="reference arm: cases of the workload run on the CPU (spread over the case ids)")
     ap.add_argument("--cases", type=int, default=None,
                     help="ws-* workloads: number of cases (default: the configuration's 64)")
