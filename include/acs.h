@@ -221,7 +221,7 @@ enum acs_option {
                                 1: CUDA graph of per-stage kernels with a device WHILE node;
                                 2: tile engine, ACS_ARITH_FAST only (ACS_E_UNSUPPORTED otherwise):
                                    32 x 32-node tiles of every active case loaded into shared
-                                   memory by TMA, four kernels per pseudo-iteration in a CUDA graph
+                                   memory by TMA, four stage kernels per pseudo-iteration in a CUDA graph
                                    with a device WHILE node -- the fastest for many cases.  Setting
                                    it builds the tile table and tensor maps (device memory).  With
                                    the environment variable ACS_NO_CONDITIONAL_GRAPH set, engines 1

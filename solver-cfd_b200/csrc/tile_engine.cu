@@ -1,5 +1,5 @@
-// tile_engine.cu -- the tile engine: one pseudo-iteration of every active case as four launches
-// over 32 x 32-node tiles whose inputs are loaded into shared memory by TMA.
+// tile_engine.cu -- the tile engine: one pseudo-iteration of every active case as four stage
+// kernels over 32 x 32-node tiles whose inputs are loaded into shared memory by TMA.
 //
 //   k_te_uv<1..3>: Runge-Kutta stage s of solve_U and of solve_V (equations.f90:244-301 and
 //                  :546-603) side by side: the stage inputs (u_in, v_in) and the arrays read with

@@ -1,8 +1,9 @@
 // tile_engine.h -- host interface of the tile engine (tile_engine.cu).
 //
-// One pseudo-iteration of every active case of a batch is five kernel launches over a table of
-// 32 x 32-node tiles covering all cases: three Runge-Kutta stages of U and V side by side, then P
-// with the three stages of T and of C, then the loop control of control.cu.  Each launch loads
+// One pseudo-iteration of every active case of a batch is four stage kernels over a table of
+// 32 x 32-node tiles covering all cases -- three Runge-Kutta stages of U and V side by side, then
+// P with the three stages of T and of C -- plus the bcUV side effects for cases whose tau arrays
+// were uploaded (after stage 1) and the loop control of control.cu.  Each stage kernel loads
 // its tiles' stencil inputs into shared memory with TMA (2-D tensor maps over the case arrays,
 // zero fill outside), computes the stage, applies the boundary passes to the tile in shared
 // memory and stores the whole tile.  FAST arithmetic only.
