@@ -67,6 +67,11 @@ ENGINES = {"cluster": 0, "graph": 1, "tile": 2}
 # u_in, v_in, um_tau, vm_tau, pn, um, vm, T (8 x 8 B) and the porous indicator (1 B, as in the
 # fused model), writes u_out, v_out (2 x 8 B)
 TILE_UV_BYTES = 8 * 8 + 1 + 2 * 8
+# DRAM bytes per node of one k_te_uv<2> launch, measured by ncu on the 64-case ws-153 workload
+# (dram__bytes_read.sum + dram__bytes_write.sum = 111,727,616 + 8,363,520 bytes for 1,498,176
+# nodes, one pass; the command is in profiles/tile_engine_ws153_ncu.md).  Other case counts are
+# scaled by their nodes.
+TILE_UV2_DRAM_BYTES_PER_NODE = (111727616 + 8363520) / 1498176
 
 
 def measured_peaks():
@@ -602,9 +607,13 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
             achieved = b_node * nodes / (k_ms * 1e-3) / 1e9
             roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst)" if peak_kind == "measured" else "fallback",
-                    "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                    "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": TILE_UV2_DRAM_BYTES_PER_NODE * nodes if args.engine == "tile" else None,
                     "bytes_per_node": b_node, "nodes_per_launch": nodes, "ms_per_launch": k_ms,
-                    "traffic_note": "DRAM bytes per launch are measured by ncu (profiles/), not inside this run"}
+                    "traffic_note": ("bytes per launch: dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                     "ncu capture of k_te_uv<2> on the 64-case workload (80.2 B per node), "
+                                     "scaled by this run's nodes" if args.engine == "tile" else
+                                     "not captured for this engine")}
         else:
             roof = {"bound": "hbm", "kernel": "k_engine (persistent cluster engine)", "achieved": loop_gbs,
                     "peak": peak, "unit": "GB/s", "frac": loop_gbs / peak, "traffic": None,
