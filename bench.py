@@ -654,6 +654,10 @@ def run_ws(args, pkg, items, kind, world, rank, dev, stream):
             "plain_gpu": {"value": plain_value, "unit": "steps/s", "steps": m, "ms_per_step": el_pl / m * 1e3,
                           "launch": f"acs_batch_run over the first {m} timed steps in one launch",
                           "pseudo_iterations_per_step_mean": float(it_pl.mean()),
+                          # the same steps of the cases the reference arm converges on the CPU (its
+                          # config.pseudo_iterations_per_step holds the oracle's counts of them)
+                          "pseudo_iterations_of_reference_cases": {
+                              str(c): [int(v) for v in it_pl[c]] for c in reference_picks(n_cases, args.ref_cases)},
                           "warm_start_value_same_steps": warm_m_value,
                           "speedup_of_warm_start": warm_m_value / plain_value,
                           "warm_pseudo_iterations_per_step_mean_same_steps": float(iters_ws[:, :m].mean()),
@@ -699,6 +703,12 @@ def _oracle_items(args):
     return items, kind
 
 
+def reference_picks(n: int, ref_cases: int) -> list:
+    """The case ids the reference arm converges on the CPU: ref_cases of the n, spread evenly."""
+    ns = max(1, min(ref_cases, n))
+    return sorted({int(round(q * (n - 1) / max(1, ns - 1))) for q in range(ns)}) if ns > 1 else [0]
+
+
 def run_reference(args):
     """The reference's CPU implementation of the loop on the host cores: the oracle, a C++
     restatement of OpenMp_Multicore/main.f90:116-186 and equations.f90 (the Fortran sources
@@ -715,8 +725,7 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     orc.set_threads(threads)
     n = len(items)
-    ns = max(1, min(args.ref_cases, n))
-    picks = sorted({int(round(q * (n - 1) / max(1, ns - 1))) for q in range(ns)}) if ns > 1 else [0]
+    picks = reference_picks(n, args.ref_cases)
     n_steps = max(1, min(args.steps, args.sample_steps))
     t_all = time.perf_counter()
     secs = 0.0
