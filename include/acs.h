@@ -187,9 +187,10 @@ int acs_batch_run(acs_batch* b, int n_steps, int* itc, int* iters, double* err, 
  * kernel of the pseudo-iteration over every case of the batch with CUDA events on the batch's
  * stream and writes the mean duration of one launch in milliseconds.  kernel: 0 = u-momentum
  * (first stage, or the whole fused routine on the FAST path), 1 = v-momentum, 2 = pressure,
- * 3 = temperature, 4 = concentration.  Only stage scratch is written (the pressure kernel's
- * output buffer is saved and restored), so the loop state is unchanged.  *cells receives the
- * nodes one launch updates. */
+ * 3 = temperature, 4 = concentration (per-stage kernels); 5 = the tile engine's U/V Runge-Kutta
+ * stage 2, 6 = its P/T/C kernel (FAST batches; sets the tile engine up if needed).  Only stage
+ * scratch is written (the output buffers of the pressure and P/T/C kernels are saved and
+ * restored), so the loop state is unchanged.  *cells receives the nodes one launch updates. */
 int acs_batch_time_kernel(acs_batch* b, int kernel, int reps, double* ms_mean, long long* cells);
 
 /* ---- solve_U without device allocation --------------------------------------------------------
