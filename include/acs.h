@@ -10,7 +10,10 @@
  *   solve_C   equations.f90:769-819   ->  acs_solve_c
  *   bcUV/bcP/bcZ/bcC boundary.f90:1-159 (called inside the routines above, as in the reference)
  *   pseudo loop + convergence check main.f90:116-186 -> acs_physical_steps / acs_batch_run
- *   mesh      nonsymetric_mesh.f90:1-218 -> acs_mesh_reference (driver-side helper)
+ *   mesh      nonsymetric_mesh.f90:1-218 -> acs_mesh_reference, acs_mesh_channel (host helpers),
+ *             acs_mesh_channel_device (device arrays)
+ *   comp_mean comp_mean.f90:1-25 (+ the velocity magnitude of transient.f90:69-74)
+ *             -> acs_cell_fields / acs_batch_cell_fields
  *
  * Conventions (those of the Fortran caller):
  *   - every field is a caller-owned host array in Fortran order (column-major, i fastest):
